@@ -1,0 +1,892 @@
+// Host runtime behind the C ABI (include/fslbm.h): contexts, solves, statistics, the batched
+// ensemble and the device-side monitor log. The reference keeps all of this in main()
+// (FSLBM.cu:489-905); here it is a library with explicit error codes.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+using namespace fslbm;
+
+// ------------------------------------------------------------------------------------------
+// errors
+// ------------------------------------------------------------------------------------------
+static thread_local std::string g_err;
+static thread_local int g_err_code = 0;
+
+int fslbm_set_error(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  g_err_code = code;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                     \
+  do {                                                                                     \
+    cudaError_t e_ = (expr);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return fslbm_set_error(FSLBM_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(e_)); \
+  } while (0)
+
+extern "C" const char* fslbm_version(void) { return "fslbm-b200 0.1"; }
+
+extern "C" int fslbm_last_error(char* buf, size_t n) {
+  if (buf && n) {
+    std::strncpy(buf, g_err.c_str(), n - 1);
+    buf[n - 1] = 0;
+  }
+  return g_err_code;
+}
+
+// ------------------------------------------------------------------------------------------
+// context
+// ------------------------------------------------------------------------------------------
+struct fslbm_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sm_count = 0;
+};
+
+extern "C" int fslbm_ctx_create(int device, fslbm_ctx** out) {
+  if (!out) return fslbm_set_error(FSLBM_ERR_ARG, "ctx_create: null output");
+  int n = 0;
+  CUDA_TRY(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n)
+    return fslbm_set_error(FSLBM_ERR_ARG, "ctx_create: device %d of %d", device, n);
+  CUDA_TRY(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10)
+    return fslbm_set_error(FSLBM_ERR_ARG, "ctx_create: device %d is sm_%d%d; this build targets sm_100a",
+                           device, prop.major, prop.minor);
+  auto* c = new fslbm_ctx;
+  c->device = device;
+  c->sm_count = prop.multiProcessorCount;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e) {
+    delete c;
+    return fslbm_set_error(FSLBM_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+  }
+  *out = c;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_ctx_destroy(fslbm_ctx* c) {
+  if (!c) return FSLBM_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return FSLBM_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// tensor-map encoding through the driver entry point (no link-time libcuda dependency)
+// ------------------------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// ------------------------------------------------------------------------------------------
+// solve
+// ------------------------------------------------------------------------------------------
+struct fslbm_solve {
+  fslbm_ctx* ctx = nullptr;
+  int lx = 0, ly = 0, L = 0, lxp = 0, d2 = 10;
+  double radius = 0, cx = 0, cy = 0;
+  int dtype = FSLBM_F32;
+  size_t es = 4;
+  fslbm_params prm{};
+  std::vector<uint8_t> mask;   // lxp*ly, padded columns are wall
+  int64_t fluid2d = 0;
+  int sx = 0, sy = 0, sz = 0;  // monitor sample cell
+  // device
+  void* state[2] = {nullptr, nullptr};
+  int cur = 0;
+  uint8_t* d_mask = nullptr;
+  void* d_colcoef = nullptr;
+  int2* d_tiles = nullptr;
+  int ntiles = 0, chunk = 0, nchunks = 0;
+  CUtensorMap maps[2];
+  DevCounters* d_counters = nullptr;
+  fslbm_monitor* d_log = nullptr;
+  int log_cap = 4096;
+  int64_t drained = 0;
+  double* d_gauge = nullptr;
+  unsigned* d_err = nullptr;
+  double* d_scratch = nullptr;     // small reductions
+  double* d_stats = nullptr;       // 11 * ly * (L + 2 d2)
+  int cnt = 0, cnt2 = 0;
+  double* d_prof = nullptr;        // 10 * lxp * ly
+  int64_t prof_n = 0;
+  void* d_stage = nullptr;         // conversion staging (dense 4 fields)
+  size_t stage_bytes = 0;
+  float* d_plane = nullptr;        // plane gather buffer
+  int64_t steps = 0;
+  bool fields_set = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0;
+  int64_t bytes_device = 0;
+  int64_t launches = 0;            // kernels launched by this solve
+  bool timing = false;             // bracket every step launch with events
+  std::vector<cudaEvent_t> tev;    // event pairs of the launches since the last read
+  size_t tev_used = 0;
+};
+
+static size_t field_stride(const fslbm_solve* s) { return size_t(s->lxp) * s->ly * s->L; }
+
+static int validate_params(const fslbm_params* p, int dtype) {
+  if (!p) return fslbm_set_error(FSLBM_ERR_ARG, "params: null");
+  if (!step_supported(dtype, p->d1))
+    return fslbm_set_error(FSLBM_ERR_ARG, "params: d1=%d is not supported for dtype %d", p->d1, dtype);
+  if (!std::isfinite(p->tblend) || !std::isfinite(p->pin) || !std::isfinite(p->nu) ||
+      !std::isfinite(p->blend))
+    return fslbm_set_error(FSLBM_ERR_ARG, "params: non-finite value");
+  if (p->monitor_every < 0) return fslbm_set_error(FSLBM_ERR_ARG, "params: monitor_every < 0");
+  if (p->delta < 0 || p->delta > 2) return fslbm_set_error(FSLBM_ERR_ARG, "params: delta must be 0, 1 or 2");
+  return FSLBM_OK;
+}
+
+static int build_tensor_maps(fslbm_solve* s) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return fslbm_set_error(FSLBM_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+  int sw, sh, hx, hy;
+  if (!step_box(s->dtype, s->prm.d1, &sw, &sh, &hx, &hy))
+    return fslbm_set_error(FSLBM_ERR_ARG, "no step kernel for dtype %d d1 %d", s->dtype, s->prm.d1);
+  const CUtensorMapDataType dt =
+      s->dtype == FSLBM_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  for (int b = 0; b < 2; ++b) {
+    cuuint64_t dims[4] = {cuuint64_t(s->lxp), cuuint64_t(s->ly), cuuint64_t(s->L), 4};
+    cuuint64_t strides[3] = {cuuint64_t(s->lxp) * s->es, cuuint64_t(s->lxp) * s->ly * s->es,
+                             cuuint64_t(field_stride(s)) * s->es};
+    cuuint32_t box[4] = {cuuint32_t(sw), cuuint32_t(sh), 1, 4};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(&s->maps[b], dt, 4, s->state[b], dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+      return fslbm_set_error(FSLBM_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
+  }
+  return FSLBM_OK;
+}
+
+// Static wall sums per column (see step_kernel.cuh): sums of w(cx)w(cy) cx^a cy^b over the
+// wall cells of the 3x3 cross-section neighbourhood; outside the box counts as wall.
+template <class TC>
+static std::vector<ColCoef<TC>> column_coefs(const fslbm_solve* s) {
+  std::vector<ColCoef<TC>> cc(size_t(s->lxp) * s->ly);
+  const double wv[3] = {1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0};
+  for (int y = 0; y < s->ly; ++y)
+    for (int x = 0; x < s->lxp; ++x) {
+      double a = 0, bx = 0, by = 0;
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int gx = x + dx, gy = y + dy;
+          const bool wall = gx < 0 || gy < 0 || gx >= s->lxp || gy >= s->ly ||
+                            s->mask[size_t(gy) * s->lxp + gx] == kWall;
+          if (!wall) continue;
+          const double w = wv[dx + 1] * wv[dy + 1];
+          a += w; bx += dx * w; by += dy * w;
+        }
+      ColCoef<TC>& c = cc[size_t(y) * s->lxp + x];
+      c.ws0 = TC(a); c.wsx = TC(bx); c.wsy = TC(by);
+      c.fluid = TC(s->mask[size_t(y) * s->lxp + x] == 0 ? 1 : 0);
+    }
+  return cc;
+}
+
+// Picks the streamwise chunking: minimises waves * (chunk + 2R) over chunk counts.
+static void choose_chunks(fslbm_solve* s) {
+  int occ = 1;
+  const size_t smem = step_smem_bytes(s->dtype, s->prm.d1);
+  occ = s->dtype == FSLBM_F64 ? 1 : 2;
+  if (smem * occ > 227 * 1024) occ = 1;
+  const int slots = std::max(1, s->ctx->sm_count * occ);
+  const int R = 2 * s->prm.d1;
+  double best = 1e300;
+  int best_n = 1;
+  for (int n = 1; n <= s->L; ++n) {
+    const int chunk = (s->L + n - 1) / n;
+    if (n > 1 && chunk < 2 * R) break;
+    const int ctas = s->ntiles * n;
+    const int waves = (ctas + slots - 1) / slots;
+    const double t = double(waves) * double(chunk + 2 * R);
+    if (t < best - 1e-9) { best = t; best_n = n; }
+  }
+  s->nchunks = best_n;
+  s->chunk = (s->L + best_n - 1) / best_n;
+  s->nchunks = (s->L + s->chunk - 1) / s->chunk;
+}
+
+static void free_solve(fslbm_solve* s) {
+  if (!s) return;
+  cudaSetDevice(s->ctx->device);
+  void* ptrs[] = {s->state[0], s->state[1], s->d_mask, s->d_colcoef, s->d_tiles, s->d_counters,
+                  s->d_log, s->d_gauge, s->d_err, s->d_scratch, s->d_stats, s->d_prof,
+                  s->d_stage, s->d_plane};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  for (cudaEvent_t e : s->tev) cudaEventDestroy(e);
+  delete s;
+}
+
+template <class T>
+static cudaError_t dalloc(fslbm_solve* s, T** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
+  if (!e) s->bytes_device += int64_t(bytes);
+  return e;
+}
+
+extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const fslbm_params* prm,
+                                  fslbm_dtype dtype, fslbm_solve** out) {
+  if (!ctx || !dom || !out) return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: null argument");
+  if (dtype != FSLBM_F32 && dtype != FSLBM_F64)
+    return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: dtype %d is not available", int(dtype));
+  int rc = validate_params(prm, dtype);
+  if (rc) return rc;
+  if (dom->lx < 3 || dom->ly < 3 || dom->lz < 1)
+    return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: box %dx%dx%d too small", dom->lx, dom->ly, dom->lz);
+  const int R = 2 * prm->d1;
+  if (dom->lz < std::max(R, 1) + 1)
+    return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: streamwise period %d shorter than the stencil reach %d",
+                           dom->lz, R + 1);
+  if (dom->buffer_depth < 0 || (dom->buffer_depth > 0 && dom->buffer_depth > dom->lz))
+    return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: buffer_depth %d out of range", dom->buffer_depth);
+  CUDA_TRY(cudaSetDevice(ctx->device));
+
+  auto* s = new fslbm_solve;
+  s->ctx = ctx;
+  s->lx = dom->lx; s->ly = dom->ly; s->L = dom->lz;
+  s->lxp = (dom->lx + 7) / 8 * 8;
+  s->d2 = dom->buffer_depth;
+  s->dtype = dtype;
+  s->es = dtype == FSLBM_F64 ? 8 : 4;
+  s->prm = *prm;
+  s->mask.assign(size_t(s->lxp) * s->ly, kWall);
+  double sxs = 0, sys = 0;
+  for (int y = 0; y < s->ly; ++y)
+    for (int x = 0; x < s->lx; ++x) {
+      uint8_t v;
+      if (dom->mask) {
+        v = dom->mask[size_t(y) * s->lx + x];
+        if (v != 0 && v != kWall) {
+          free_solve(s);
+          return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: mask value %d at (%d,%d); expected 0 or 125", v, x, y);
+        }
+      } else {
+        const double dx = x - dom->cx, dy = y - dom->cy;
+        v = (dx * dx + dy * dy <= dom->radius * dom->radius) ? 0 : kWall;
+      }
+      if (v == 0 && (x == 0 || y == 0 || x == s->lx - 1 || y == s->ly - 1)) {
+        free_solve(s);
+        return fslbm_set_error(FSLBM_ERR_ARG,
+                               "solve_create: fluid cell (%d,%d) on the box rim; the cross-section must be "
+                               "enclosed by wall", x, y);
+      }
+      s->mask[size_t(y) * s->lxp + x] = v;
+      if (v == 0) { ++s->fluid2d; sxs += x; sys += y; }
+    }
+  if (s->fluid2d == 0) {
+    free_solve(s);
+    return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: no fluid cells");
+  }
+  s->radius = dom->radius > 0 ? dom->radius : std::sqrt(double(s->fluid2d) / M_PI);
+  s->cx = dom->mask ? sxs / s->fluid2d : dom->cx;
+  s->cy = dom->mask ? sys / s->fluid2d : dom->cy;
+  // monitor sample: linear index (ly*lx)/2 + lx/2 of the plane z = lz_ref/2 (FSLBM.cu:653,665)
+  {
+    const long idx = (long(s->ly) * s->lx) / 2 + s->lx / 2;
+    s->sx = int(idx % s->lx);
+    s->sy = int(idx / s->lx);
+    if (s->sy >= s->ly) s->sy = s->ly - 1;
+    s->sz = s->L / 2;
+  }
+  // tiles that contain fluid
+  std::vector<int2> tiles;
+  for (int y0 = 0; y0 < s->ly; y0 += kTY)
+    for (int x0 = 0; x0 < s->lxp; x0 += kTX) {
+      bool any = false;
+      for (int y = y0; y < std::min(y0 + kTY, s->ly) && !any; ++y)
+        for (int x = x0; x < std::min(x0 + kTX, s->lxp); ++x)
+          if (s->mask[size_t(y) * s->lxp + x] == 0) { any = true; break; }
+      if (any) tiles.push_back(make_int2(x0, y0));
+    }
+  s->ntiles = int(tiles.size());
+
+  const size_t fs = field_stride(s);
+  cudaError_t e = cudaSuccess;
+  auto fail = [&](const char* what) {
+    const int r = fslbm_set_error(FSLBM_ERR_CUDA, "solve_create: %s: %s", what, cudaGetErrorString(e));
+    free_solve(s);
+    return r;
+  };
+  for (int b = 0; b < 2; ++b) {
+    if ((e = dalloc(s, &s->state[b], 4 * fs * s->es))) return fail("state");
+    if ((e = cudaMemset(s->state[b], 0, 4 * fs * s->es))) return fail("memset");
+  }
+  if ((e = dalloc(s, &s->d_mask, s->mask.size()))) return fail("mask");
+  cudaMemcpy(s->d_mask, s->mask.data(), s->mask.size(), cudaMemcpyHostToDevice);
+  if (dtype == FSLBM_F64) {
+    auto cc = column_coefs<double>(s);
+    if ((e = dalloc(s, &s->d_colcoef, cc.size() * sizeof(cc[0])))) return fail("colcoef");
+    cudaMemcpy(s->d_colcoef, cc.data(), cc.size() * sizeof(cc[0]), cudaMemcpyHostToDevice);
+  } else {
+    auto cc = column_coefs<float>(s);
+    if ((e = dalloc(s, &s->d_colcoef, cc.size() * sizeof(cc[0])))) return fail("colcoef");
+    cudaMemcpy(s->d_colcoef, cc.data(), cc.size() * sizeof(cc[0]), cudaMemcpyHostToDevice);
+  }
+  if ((e = dalloc(s, &s->d_tiles, tiles.size() * sizeof(int2)))) return fail("tiles");
+  cudaMemcpy(s->d_tiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice);
+  if ((e = dalloc(s, &s->d_counters, sizeof(DevCounters)))) return fail("counters");
+  cudaMemset(s->d_counters, 0, sizeof(DevCounters));
+  if ((e = dalloc(s, &s->d_log, sizeof(fslbm_monitor) * s->log_cap))) return fail("log");
+  if ((e = dalloc(s, &s->d_gauge, sizeof(double)))) return fail("gauge");
+  cudaMemset(s->d_gauge, 0, sizeof(double));
+  if ((e = dalloc(s, &s->d_err, sizeof(unsigned)))) return fail("err");
+  cudaMemset(s->d_err, 0, sizeof(unsigned));
+  if ((e = dalloc(s, &s->d_scratch, 8 * sizeof(double)))) return fail("scratch");
+  if ((e = cudaEventCreate(&s->ev0)) || (e = cudaEventCreate(&s->ev1))) return fail("events");
+  if ((e = step_prepare(dtype, prm->d1))) return fail("step_prepare");
+  if (int r = build_tensor_maps(s)) { free_solve(s); return r; }
+  choose_chunks(s);
+  if ((e = cudaDeviceSynchronize())) return fail("set-up");
+  *out = s;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_solve_destroy(fslbm_solve* s) {
+  free_solve(s);
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_solve_set_params(fslbm_solve* s, const fslbm_params* prm) {
+  if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "set_params: null solve");
+  int rc = validate_params(prm, s->dtype);
+  if (rc) return rc;
+  const bool d1_changed = prm->d1 != s->prm.d1;
+  s->prm = *prm;
+  if (d1_changed) {
+    CUDA_TRY(cudaSetDevice(s->ctx->device));
+    CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+    CUDA_TRY(step_prepare(s->dtype, prm->d1));
+    if (int r = build_tensor_maps(s)) return r;
+    choose_chunks(s);
+  }
+  return FSLBM_OK;
+}
+
+static int ensure_stage(fslbm_solve* s, size_t bytes) {
+  if (s->stage_bytes >= bytes) return FSLBM_OK;
+  if (s->d_stage) {
+    cudaFree(s->d_stage);
+    s->bytes_device -= int64_t(s->stage_bytes);
+    s->d_stage = nullptr;
+    s->stage_bytes = 0;
+  }
+  CUDA_TRY(dalloc(s, &s->d_stage, bytes));
+  s->stage_bytes = bytes;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_solve_set_fields(fslbm_solve* s, fslbm_dtype hd, const void* p, const void* u,
+                                      const void* v, const void* w) {
+  if (!s || !p || !u || !v || !w) return fslbm_set_error(FSLBM_ERR_ARG, "set_fields: null argument");
+  if (hd != FSLBM_F64 && hd != FSLBM_F32)
+    return fslbm_set_error(FSLBM_ERR_ARG, "set_fields: host dtype must be F64 or F32");
+  CUDA_TRY(cudaSetDevice(s->ctx->device));
+  const size_t n = size_t(s->lx) * s->ly * s->L, hes = hd == FSLBM_F64 ? 8 : 4;
+  cudaStream_t st = s->ctx->stream;
+  void* dst = s->state[s->cur];
+  if (int(hd) == s->dtype) {
+    // same type: pitched copies straight into the state
+    const void* src[4] = {p, u, v, w};
+    for (int f = 0; f < 4; ++f)
+      CUDA_TRY(cudaMemcpy2DAsync(static_cast<char*>(dst) + f * field_stride(s) * s->es,
+                                 size_t(s->lxp) * s->es, src[f], size_t(s->lx) * hes,
+                                 size_t(s->lx) * hes, size_t(s->ly) * s->L,
+                                 cudaMemcpyHostToDevice, st));
+  } else {
+    if (int r = ensure_stage(s, 4 * n * hes)) return r;
+    const void* src[4] = {p, u, v, w};
+    for (int f = 0; f < 4; ++f)
+      CUDA_TRY(cudaMemcpyAsync(static_cast<char*>(s->d_stage) + f * n * hes, src[f], n * hes,
+                               cudaMemcpyHostToDevice, st));
+    CUDA_TRY(launch_convert_in(s->dtype, dst, s->d_stage, hd == FSLBM_F64, s->lx, s->lxp, s->ly,
+                               s->L, st));
+  }
+  CUDA_TRY(launch_zero_walls(s->dtype, dst, s->d_mask, s->lxp, s->ly, s->L, st));
+  // the other buffer's walls (never written by the step) must be zero too
+  CUDA_TRY(launch_zero_walls(s->dtype, s->state[1 - s->cur], s->d_mask, s->lxp, s->ly, s->L, st));
+  s->fields_set = true;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_solve_get_fields(fslbm_solve* s, fslbm_dtype hd, void* p, void* u, void* v,
+                                      void* w) {
+  if (!s || !p || !u || !v || !w) return fslbm_set_error(FSLBM_ERR_ARG, "get_fields: null argument");
+  if (hd != FSLBM_F64 && hd != FSLBM_F32)
+    return fslbm_set_error(FSLBM_ERR_ARG, "get_fields: host dtype must be F64 or F32");
+  CUDA_TRY(cudaSetDevice(s->ctx->device));
+  const size_t n = size_t(s->lx) * s->ly * s->L, hes = hd == FSLBM_F64 ? 8 : 4;
+  cudaStream_t st = s->ctx->stream;
+  const void* src = s->state[s->cur];
+  void* dst[4] = {p, u, v, w};
+  if (int(hd) == s->dtype) {
+    for (int f = 0; f < 4; ++f)
+      CUDA_TRY(cudaMemcpy2DAsync(dst[f], size_t(s->lx) * hes,
+                                 static_cast<const char*>(src) + f * field_stride(s) * s->es,
+                                 size_t(s->lxp) * s->es, size_t(s->lx) * hes,
+                                 size_t(s->ly) * s->L, cudaMemcpyDeviceToHost, st));
+  } else {
+    if (int r = ensure_stage(s, 4 * n * hes)) return r;
+    CUDA_TRY(launch_convert_out(s->dtype, src, s->d_stage, hd == FSLBM_F64, s->lx, s->lxp, s->ly,
+                                s->L, st));
+    for (int f = 0; f < 4; ++f)
+      CUDA_TRY(cudaMemcpyAsync(dst[f], static_cast<char*>(s->d_stage) + f * n * hes, n * hes,
+                               cudaMemcpyDeviceToHost, st));
+  }
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return FSLBM_OK;
+}
+
+// Per-step constants formed as the reference forms them (FSLBM.cu:231, 269, 599, 624): in the
+// storage precision for FP32, in FP64 otherwise.
+static void fill_constants(const fslbm_solve* s, StepLaunch& a) {
+  const fslbm_params& p = s->prm;
+  if (s->dtype == FSLBM_F32) {
+    const float tb = float(p.tblend), nu = float(p.nu), blend = float(p.blend);
+    a.tb = tb;
+    a.cc = float(1.0 - double(tb));
+    a.pin = float(p.pin);
+    a.dtddy = nu - 0.16666666f;
+    a.m = float(1.0 / double(float(p.d1 * p.d1)));
+    a.c0 = -6.0f - 1.5f * blend;
+    a.c1 = 1.0f + 0.3333333333f * blend;
+    a.c2 = -0.0833333333f * blend;
+    a.fx = float(p.force[0]); a.fy = float(p.force[1]); a.fz = float(p.force[2]);
+  } else {
+    a.tb = p.tblend;
+    a.cc = 1.0 - p.tblend;
+    a.pin = p.pin;
+    a.dtddy = p.nu - 0.16666666;
+    a.m = 1.0 / double(p.d1 * p.d1);
+    a.c0 = -6.0 - 1.5 * p.blend;
+    a.c1 = 1.0 + 0.3333333333 * p.blend;
+    a.c2 = -0.0833333333 * p.blend;
+    a.fx = p.force[0]; a.fy = p.force[1]; a.fz = p.force[2];
+  }
+}
+
+static int enqueue_steps(fslbm_solve* s, int64_t nsteps) {
+  cudaStream_t st = s->ctx->stream;
+  StepLaunch a{};
+  a.dtype = s->dtype; a.d1 = s->prm.d1;
+  a.lxp = s->lxp; a.ly = s->ly; a.L = s->L;
+  a.ntiles = s->ntiles; a.chunk = s->chunk; a.nchunks = s->nchunks;
+  a.tiles = s->d_tiles; a.mask = s->d_mask; a.colcoef = s->d_colcoef;
+  a.err = s->d_err; a.counters = s->d_counters;
+  fill_constants(s, a);
+  MonitorLaunch m{};
+  m.dtype = s->dtype; m.mask = s->d_mask;
+  m.lxp = s->lxp; m.lx = s->lx; m.ly = s->ly; m.L = s->L;
+  m.pin = s->dtype == FSLBM_F32 ? double(float(s->prm.pin)) : s->prm.pin;
+  m.nu = s->prm.nu; m.radius = s->radius; m.l1 = double(s->fluid2d);
+  m.sx = s->sx; m.sy = s->sy; m.sz = s->sz;
+  m.log = s->d_log; m.log_cap = s->log_cap; m.gauge_out = s->d_gauge; m.counters = s->d_counters;
+  const int me = s->prm.monitor_every;
+  for (int64_t n = 0; n < nsteps; ++n) {
+    const int64_t c = s->steps + 1;
+    a.map = &s->maps[s->cur];
+    a.out = s->state[1 - s->cur];
+    a.gauge = (me > 0 && c > 1 && (c - 1) % me == 0) ? s->d_gauge : nullptr;
+    if (s->timing) {
+      while (s->tev.size() < s->tev_used + 2) {
+        cudaEvent_t e;
+        CUDA_TRY(cudaEventCreate(&e));
+        s->tev.push_back(e);
+      }
+      CUDA_TRY(cudaEventRecord(s->tev[s->tev_used], st));
+    }
+    CUDA_TRY(launch_step(a, st));
+    if (s->timing) {
+      CUDA_TRY(cudaEventRecord(s->tev[s->tev_used + 1], st));
+      s->tev_used += 2;
+    }
+    ++s->launches;
+    s->cur ^= 1;
+    s->steps = c;
+    if (me > 0 && c % me == 0) {
+      m.state = s->state[s->cur];
+      CUDA_TRY(launch_monitor(m, st));
+      ++s->launches;
+    }
+  }
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_solve_step(fslbm_solve* s, int64_t nsteps) {
+  if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "step: null solve");
+  if (nsteps < 0) return fslbm_set_error(FSLBM_ERR_ARG, "step: negative step count");
+  if (!s->fields_set) return fslbm_set_error(FSLBM_ERR_STATE, "step: fields were never set");
+  CUDA_TRY(cudaSetDevice(s->ctx->device));
+  CUDA_TRY(cudaEventRecord(s->ev0, s->ctx->stream));
+  if (int r = enqueue_steps(s, nsteps)) return r;
+  CUDA_TRY(cudaEventRecord(s->ev1, s->ctx->stream));
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_solve_sync(fslbm_solve* s) {
+  if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "sync: null solve");
+  CUDA_TRY(cudaSetDevice(s->ctx->device));
+  CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, s->ev0, s->ev1) == cudaSuccess) s->last_ms = ms;
+  unsigned err = 0;
+  CUDA_TRY(cudaMemcpy(&err, s->d_err, sizeof err, cudaMemcpyDeviceToHost));
+  if (err) {
+    cudaMemset(s->d_err, 0, sizeof(unsigned));
+    return fslbm_set_error(FSLBM_ERR_TIMEOUT, "a bounded device wait gave up (flags 0x%x)", err);
+  }
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_solve_monitor_log(fslbm_solve* s, fslbm_monitor* out, int max, int* n_out) {
+  if (!s || (!out && max > 0)) return fslbm_set_error(FSLBM_ERR_ARG, "monitor_log: null argument");
+  if (int r = fslbm_solve_sync(s)) return r;
+  DevCounters c;
+  CUDA_TRY(cudaMemcpy(&c, s->d_counters, sizeof c, cudaMemcpyDeviceToHost));
+  int64_t first = std::max<int64_t>(s->drained, c.records - s->log_cap);
+  int n = 0;
+  for (int64_t k = first; k < c.records && n < max; ++k, ++n)
+    CUDA_TRY(cudaMemcpy(&out[n], s->d_log + (k % s->log_cap), sizeof(fslbm_monitor),
+                        cudaMemcpyDeviceToHost));
+  s->drained = first + n;
+  if (n_out) *n_out = n;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_solve_monitor(fslbm_solve* s, fslbm_monitor* out) {
+  if (!s || !out) return fslbm_set_error(FSLBM_ERR_ARG, "monitor: null argument");
+  if (int r = fslbm_solve_sync(s)) return r;
+  DevCounters c;
+  CUDA_TRY(cudaMemcpy(&c, s->d_counters, sizeof c, cudaMemcpyDeviceToHost));
+  if (c.records == 0) return fslbm_set_error(FSLBM_ERR_STATE, "monitor: no record yet");
+  CUDA_TRY(cudaMemcpy(out, s->d_log + ((c.records - 1) % s->log_cap), sizeof(fslbm_monitor),
+                      cudaMemcpyDeviceToHost));
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_solve_check(fslbm_solve* s, double* max_abs_u) {
+  if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "check: null solve");
+  CUDA_TRY(cudaSetDevice(s->ctx->device));
+  CUDA_TRY(launch_check(s->dtype, s->state[s->cur], field_stride(s), s->d_scratch, s->ctx->stream));
+  double r[2];
+  CUDA_TRY(cudaMemcpyAsync(r, s->d_scratch, sizeof r, cudaMemcpyDeviceToHost, s->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+  if (max_abs_u) *max_abs_u = r[1];
+  if (r[0] > 0)
+    return fslbm_set_error(FSLBM_ERR_DIVERGED, "check: %.0f non-finite values in the fields", r[0]);
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_solve_info(fslbm_solve* s, fslbm_info* out) {
+  if (!s || !out) return fslbm_set_error(FSLBM_ERR_ARG, "info: null argument");
+  out->cells = int64_t(s->lx) * s->ly * s->L;
+  out->fluid_cells = s->fluid2d * s->L;
+  out->bytes_device = s->bytes_device;
+  out->steps = s->steps;
+  out->lx_pitch = s->lxp;
+  out->dtype = s->dtype;
+  out->last_step_ms = s->last_ms;
+  out->kernel_launches = s->launches;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_solve_set_timing(fslbm_solve* s, int enable) {
+  if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "set_timing: null solve");
+  s->timing = enable != 0;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_solve_kernel_time(fslbm_solve* s, double* ms_total, int64_t* launches) {
+  if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "kernel_time: null solve");
+  CUDA_TRY(cudaSetDevice(s->ctx->device));
+  CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+  double t = 0;
+  for (size_t k = 0; k + 1 < s->tev_used; k += 2) {
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, s->tev[k], s->tev[k + 1]));
+    t += ms;
+  }
+  if (ms_total) *ms_total = t;
+  if (launches) *launches = int64_t(s->tev_used / 2);
+  s->tev_used = 0;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_solve_device_fields(fslbm_solve* s, void** p, void** u, void** v, void** w) {
+  if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "device_fields: null solve");
+  char* b = static_cast<char*>(s->state[s->cur]);
+  const size_t fb = field_stride(s) * s->es;
+  if (p) *p = b;
+  if (u) *u = b + fb;
+  if (v) *v = b + 2 * fb;
+  if (w) *w = b + 3 * fb;
+  return FSLBM_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// reference layout (buffer planes reconstructed as bcond copies, FSLBM.cu:291-301)
+// ------------------------------------------------------------------------------------------
+extern "C" int fslbm_solve_get_fields_ref(fslbm_solve* s, float* p, float* u, float* v, float* w) {
+  if (!s || !p || !u || !v || !w) return fslbm_set_error(FSLBM_ERR_ARG, "get_fields_ref: null argument");
+  const size_t plane = size_t(s->lx) * s->ly, n = plane * s->L;
+  std::vector<float> core(4 * n);
+  if (int r = fslbm_solve_get_fields(s, FSLBM_F32, core.data(), core.data() + n,
+                                     core.data() + 2 * n, core.data() + 3 * n))
+    return r;
+  const int d2 = s->d2, Lr = s->L + 2 * d2;
+  const float pin = float(s->prm.pin);
+  float* dst[4] = {p, u, v, w};
+  for (int zr = 0; zr < Lr; ++zr) {
+    int zc = zr - d2, jump = 0;
+    if (zc < 0) { zc += s->L; jump = 1; } else if (zc >= s->L) { zc -= s->L; jump = -1; }
+    for (int f = 0; f < 4; ++f)
+      std::memcpy(dst[f] + plane * zr, core.data() + f * n + plane * zc, plane * sizeof(float));
+    if (jump)
+      for (size_t j = 0; j < plane; ++j) {
+        const int x = int(j % s->lx), y = int(j / s->lx);
+        if (s->mask[size_t(y) * s->lxp + x] == kWall) continue;
+        float& pv = p[plane * zr + j];
+        pv = jump > 0 ? pv + pin : pv - pin;
+      }
+  }
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_solve_set_fields_ref(fslbm_solve* s, const float* p, const float* u,
+                                          const float* v, const float* w) {
+  if (!s || !p || !u || !v || !w) return fslbm_set_error(FSLBM_ERR_ARG, "set_fields_ref: null argument");
+  const size_t off = size_t(s->lx) * s->ly * s->d2;
+  return fslbm_solve_set_fields(s, FSLBM_F32, p + off, u + off, v + off, w + off);
+}
+
+extern "C" int fslbm_solve_get_plane(fslbm_solve* s, int kind, int comp, float* out) {
+  if (!s || !out || comp < 0 || comp > 3 || kind < 0 || kind > 1)
+    return fslbm_set_error(FSLBM_ERR_ARG, "get_plane: bad argument");
+  CUDA_TRY(cudaSetDevice(s->ctx->device));
+  cudaStream_t st = s->ctx->stream;
+  const int Lr = s->L + 2 * s->d2;
+  if (!s->d_plane) {
+    const size_t need = 4 * std::max(size_t(s->L) * s->ly, size_t(s->ly) * s->lx) * sizeof(float);
+    CUDA_TRY(dalloc(s, &s->d_plane, need));
+  }
+  std::vector<float> buf;
+  if (kind == 0) {
+    const int xs = s->lx / 2;
+    CUDA_TRY(launch_gather_plane(s->dtype, s->state[s->cur], s->lx, s->lxp, s->ly, s->L, 0, xs,
+                                 s->d_plane, st));
+    buf.resize(4 * size_t(s->L) * s->ly);
+    CUDA_TRY(cudaMemcpyAsync(buf.data(), s->d_plane, buf.size() * sizeof(float),
+                             cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    const size_t n = size_t(s->L) * s->ly;
+    const float pin = float(s->prm.pin);
+    for (int zr = 0; zr < Lr; ++zr) {
+      int zc = zr - s->d2, jump = 0;
+      if (zc < 0) { zc += s->L; jump = 1; } else if (zc >= s->L) { zc -= s->L; jump = -1; }
+      for (int y = 0; y < s->ly; ++y) {
+        float val = buf[comp * n + size_t(zc) * s->ly + y];
+        if (comp == 0 && jump && s->mask[size_t(y) * s->lxp + xs] != kWall)
+          val = jump > 0 ? val + pin : val - pin;
+        out[size_t(zr) * s->ly + y] = val;
+      }
+    }
+  } else {
+    int zr = Lr / 2, zc = zr - s->d2, jump = 0;
+    if (zc < 0) { zc += s->L; jump = 1; } else if (zc >= s->L) { zc -= s->L; jump = -1; }
+    CUDA_TRY(launch_gather_plane(s->dtype, s->state[s->cur], s->lx, s->lxp, s->ly, s->L, 1, zc,
+                                 s->d_plane, st));
+    const size_t n = size_t(s->ly) * s->lx;
+    buf.resize(4 * n);
+    CUDA_TRY(cudaMemcpyAsync(buf.data(), s->d_plane, buf.size() * sizeof(float),
+                             cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    const float pin = float(s->prm.pin);
+    for (size_t j = 0; j < n; ++j) {
+      float val = buf[comp * n + j];
+      const int x = int(j % s->lx), y = int(j / s->lx);
+      if (comp == 0 && jump && s->mask[size_t(y) * s->lxp + x] != kWall)
+        val = jump > 0 ? val + pin : val - pin;
+      out[j] = val;
+    }
+  }
+  return FSLBM_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// statistics
+// ------------------------------------------------------------------------------------------
+static int ensure_stats(fslbm_solve* s) {
+  if (s->d_stats) return FSLBM_OK;
+  const size_t n = size_t(s->ly) * (s->L + 2 * s->d2);
+  CUDA_TRY(dalloc(s, &s->d_stats, 11 * n * sizeof(double)));
+  CUDA_TRY(cudaMemsetAsync(s->d_stats, 0, 11 * n * sizeof(double), s->ctx->stream));
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_stats_sample(fslbm_solve* s) {
+  if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "stats_sample: null solve");
+  CUDA_TRY(cudaSetDevice(s->ctx->device));
+  if (int r = ensure_stats(s)) return r;
+  const size_t n = size_t(s->ly) * (s->L + 2 * s->d2);
+  cudaStream_t st = s->ctx->stream;
+  // reset policy (FSLBM.cu:683-690)
+  if (s->prm.delta == 0) {
+    s->cnt = 0; s->cnt2 = 0;
+    CUDA_TRY(cudaMemsetAsync(s->d_stats, 0, 11 * n * sizeof(double), st));
+  } else if (s->prm.delta == 1) {
+    s->cnt2 = 0;
+    CUDA_TRY(cudaMemsetAsync(s->d_stats + 4 * n, 0, 7 * n * sizeof(double), st));
+  }
+  s->cnt += 1; s->cnt2 += 1;                                   // FSLBM.cu:715
+  const double pin = s->dtype == FSLBM_F32 ? double(float(s->prm.pin)) : s->prm.pin;
+  CUDA_TRY(launch_plane_stats(s->dtype, s->state[s->cur], s->d_mask, s->lxp, s->ly, s->L, s->d2,
+                              s->lx / 2, pin, s->cnt, 1, 1, s->d_stats, st));
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_stats_get(fslbm_solve* s, double* out, int* cnt, int* cnt2) {
+  if (!s || !out) return fslbm_set_error(FSLBM_ERR_ARG, "stats_get: null argument");
+  CUDA_TRY(cudaSetDevice(s->ctx->device));
+  if (int r = ensure_stats(s)) return r;
+  const size_t n = size_t(s->ly) * (s->L + 2 * s->d2);
+  CUDA_TRY(cudaMemcpyAsync(out, s->d_stats, 11 * n * sizeof(double), cudaMemcpyDeviceToHost,
+                           s->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+  for (size_t k = 0; k < 4 * n; ++k) out[k] = s->cnt ? out[k] / double(s->cnt) : 0.0;
+  for (size_t k = 4 * n; k < 11 * n; ++k) out[k] = s->cnt2 ? out[k] / double(s->cnt2) : 0.0;
+  if (cnt) *cnt = s->cnt;
+  if (cnt2) *cnt2 = s->cnt2;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_stats_set(fslbm_solve* s, const double* means, int cnt, int cnt2) {
+  if (!s || !means || cnt < 0 || cnt2 < 0) return fslbm_set_error(FSLBM_ERR_ARG, "stats_set: bad argument");
+  CUDA_TRY(cudaSetDevice(s->ctx->device));
+  if (int r = ensure_stats(s)) return r;
+  const size_t n = size_t(s->ly) * (s->L + 2 * s->d2);
+  std::vector<double> sums(11 * n);
+  for (size_t k = 0; k < 4 * n; ++k) sums[k] = means[k] * double(cnt);        // FSLBM.cu:453-456
+  for (size_t k = 4 * n; k < 11 * n; ++k) sums[k] = means[k] * double(cnt2);  // FSLBM.cu:457-463
+  CUDA_TRY(cudaMemcpy(s->d_stats, sums.data(), sums.size() * sizeof(double), cudaMemcpyHostToDevice));
+  s->cnt = cnt; s->cnt2 = cnt2;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_profile_sample(fslbm_solve* s) {
+  if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "profile_sample: null solve");
+  CUDA_TRY(cudaSetDevice(s->ctx->device));
+  const size_t n = size_t(s->lxp) * s->ly;
+  if (!s->d_prof) {
+    CUDA_TRY(dalloc(s, &s->d_prof, 10 * n * sizeof(double)));
+    CUDA_TRY(cudaMemsetAsync(s->d_prof, 0, 10 * n * sizeof(double), s->ctx->stream));
+  }
+  CUDA_TRY(launch_profile(s->dtype, s->state[s->cur], s->lxp, s->ly, s->L, s->d_prof, s->ctx->stream));
+  s->prof_n += 1;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_profile_get(fslbm_solve* s, double* sums, int64_t* nsamples) {
+  if (!s || !sums) return fslbm_set_error(FSLBM_ERR_ARG, "profile_get: null argument");
+  CUDA_TRY(cudaSetDevice(s->ctx->device));
+  const size_t n = size_t(s->lxp) * s->ly;
+  std::vector<double> buf(10 * n, 0.0);
+  if (s->d_prof) {
+    CUDA_TRY(cudaMemcpyAsync(buf.data(), s->d_prof, buf.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost, s->ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+  }
+  for (int k = 0; k < 10; ++k)
+    for (int y = 0; y < s->ly; ++y)
+      for (int x = 0; x < s->lx; ++x)
+        sums[(size_t(k) * s->ly + y) * s->lx + x] = buf[(size_t(k) * s->ly + y) * s->lxp + x];
+  if (nsamples) *nsamples = s->prof_n;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_profile_reset(fslbm_solve* s) {
+  if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "profile_reset: null solve");
+  if (s->d_prof) {
+    CUDA_TRY(cudaSetDevice(s->ctx->device));
+    CUDA_TRY(cudaMemsetAsync(s->d_prof, 0, 10 * size_t(s->lxp) * s->ly * sizeof(double), s->ctx->stream));
+  }
+  s->prof_n = 0;
+  return FSLBM_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// batched ensemble (first form: the members' steps enqueued back to back on one stream)
+// ------------------------------------------------------------------------------------------
+struct fslbm_batch {
+  fslbm_ctx* ctx;
+  std::vector<fslbm_solve*> members;
+};
+
+extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, int n, fslbm_batch** out) {
+  if (!ctx || !out || n < 1 || !solves) return fslbm_set_error(FSLBM_ERR_ARG, "batch_create: bad argument");
+  auto* b = new fslbm_batch{ctx, {}};
+  for (int i = 0; i < n; ++i) {
+    if (!solves[i] || solves[i]->ctx != ctx) {
+      delete b;
+      return fslbm_set_error(FSLBM_ERR_ARG, "batch_create: member %d is null or of another context", i);
+    }
+    b->members.push_back(solves[i]);
+  }
+  *out = b;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_batch_destroy(fslbm_batch* b) {
+  delete b;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int) {
+  if (!b) return fslbm_set_error(FSLBM_ERR_ARG, "batch_step: null batch");
+  for (fslbm_solve* s : b->members)
+    if (int r = fslbm_solve_step(s, nsteps)) return r;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_batch_sync(fslbm_batch* b) {
+  if (!b) return fslbm_set_error(FSLBM_ERR_ARG, "batch_sync: null batch");
+  for (fslbm_solve* s : b->members)
+    if (int r = fslbm_solve_sync(s)) return r;
+  return FSLBM_OK;
+}

@@ -1,0 +1,259 @@
+// Host-side file formats and generators of the drop-in surface: pipe.txt and param.txt
+// (written by pipe.m, read by FSLBM.cu), the pipe.m geometry, the reference-layout mask split
+// and the seeded initial-field generator.
+#include <algorithm>
+#include <cctype>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fslbm.h"
+
+int fslbm_set_error(int code, const char* fmt, ...);
+
+namespace {
+
+constexpr uint8_t kWall = 125, kBuf = 1;
+
+bool read_file(const char* path, std::string& out) {
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return false;
+  char buf[1 << 16];
+  size_t n;
+  out.clear();
+  while ((n = std::fread(buf, 1, sizeof buf, f)) > 0) out.append(buf, n);
+  std::fclose(f);
+  return true;
+}
+
+// Splits on whitespace.
+std::vector<std::string> tokens(const std::string& s) {
+  std::vector<std::string> t;
+  size_t i = 0;
+  while (i < s.size()) {
+    while (i < s.size() && std::isspace(static_cast<unsigned char>(s[i]))) ++i;
+    size_t j = i;
+    while (j < s.size() && !std::isspace(static_cast<unsigned char>(s[j]))) ++j;
+    if (j > i) t.emplace_back(s.substr(i, j - i));
+    i = j;
+  }
+  return t;
+}
+
+bool parse_double(const std::string& t, double* v) {
+  char* end = nullptr;
+  errno = 0;
+  *v = std::strtod(t.c_str(), &end);
+  return errno == 0 && end && *end == 0;
+}
+
+bool parse_int(const std::string& t, int* v) {
+  double d;
+  if (!parse_double(t, &d) || d != std::floor(d) || std::fabs(d) > 2e9) return false;
+  *v = int(d);
+  return true;
+}
+
+uint64_t splitmix64(uint64_t x) {
+  // splitmix64 (Steele, Lea, Flood 2014): golden-ratio increment, two xor-shift-multiply rounds
+  uint64_t z = x + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// uniform in [-1, 1) from (seed, counter)
+double unit_pm(uint64_t seed, uint64_t counter) {
+  const uint64_t r = splitmix64(splitmix64(seed) ^ counter);
+  return double(r >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+}  // namespace
+
+extern "C" int fslbm_read_pipe_txt(const char* path, int lx, int ly, int lz, uint8_t* out) {
+  if (!path || !out || lx <= 0 || ly <= 0 || lz <= 0)
+    return fslbm_set_error(FSLBM_ERR_ARG, "read_pipe_txt: bad argument");
+  std::string s;
+  if (!read_file(path, s)) return fslbm_set_error(FSLBM_ERR_IO, "read_pipe_txt: cannot open %s", path);
+  const size_t n = size_t(lx) * ly * lz;
+  const std::vector<std::string> t = tokens(s);
+  if (t.size() != n)
+    return fslbm_set_error(FSLBM_ERR_IO, "read_pipe_txt: %s holds %zu values, expected %zu (%dx%dx%d)",
+                           path, t.size(), n, lx, ly, lz);
+  for (size_t i = 0; i < n; ++i) {
+    int v;
+    if (!parse_int(t[i], &v) || v < 0 || v > 255)
+      return fslbm_set_error(FSLBM_ERR_IO, "read_pipe_txt: value %zu ('%s') is not a byte", i, t[i].c_str());
+    out[i] = uint8_t(v);
+  }
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_write_pipe_txt(const char* path, int lx, int ly, int lz, const uint8_t* mask) {
+  if (!path || !mask) return fslbm_set_error(FSLBM_ERR_ARG, "write_pipe_txt: bad argument");
+  FILE* f = std::fopen(path, "w");
+  if (!f) return fslbm_set_error(FSLBM_ERR_IO, "write_pipe_txt: cannot create %s", path);
+  const size_t n = size_t(lx) * ly * lz;
+  for (size_t i = 0; i < n; ++i) std::fprintf(f, "%d\n", int(mask[i]));   // pipe.m:62
+  std::fclose(f);
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_read_param_txt(const char* path, fslbm_params* prm) {
+  if (!path || !prm) return fslbm_set_error(FSLBM_ERR_ARG, "read_param_txt: bad argument");
+  std::string s;
+  if (!read_file(path, s)) return fslbm_set_error(FSLBM_ERR_IO, "read_param_txt: cannot open %s", path);
+  const std::vector<std::string> t = tokens(s);
+  // FSLBM.cu:502-507: %e tblend, %e pin, %e nu, %d d1, %d delta, %e blend; trailing lines
+  // (the unused save path, :508) are ignored. Floats are read into FP32 as the reference does.
+  const int nval = int(std::min<size_t>(t.size(), 6));
+  fslbm_params p = *prm;
+  for (int k = 0; k < nval; ++k) {
+    if (k == 3 || k == 4) {
+      int v;
+      if (!parse_int(t[k], &v))
+        return fslbm_set_error(FSLBM_ERR_IO, "read_param_txt: line %d ('%s') is not an integer", k + 1, t[k].c_str());
+      (k == 3 ? p.d1 : p.delta) = v;
+    } else {
+      double v;
+      if (!parse_double(t[k], &v))
+        return fslbm_set_error(FSLBM_ERR_IO, "read_param_txt: line %d ('%s') is not a number", k + 1, t[k].c_str());
+      const double f = double(float(v));
+      if (k == 0) p.tblend = f;
+      else if (k == 1) p.pin = f;
+      else if (k == 2) p.nu = f;
+      else p.blend = f;
+    }
+  }
+  if (nval < 6) return fslbm_set_error(FSLBM_ERR_IO, "read_param_txt: %s holds %d of 6 values", path, nval);
+  *prm = p;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_write_param_txt(const char* path, const fslbm_params* prm) {
+  if (!path || !prm) return fslbm_set_error(FSLBM_ERR_ARG, "write_param_txt: bad argument");
+  FILE* f = std::fopen(path, "w");
+  if (!f) return fslbm_set_error(FSLBM_ERR_IO, "write_param_txt: cannot create %s", path);
+  // pipe.m:67-68 writes '%f\n%f\n%f\n%d\n%d\n' and recycles '%f\n' for the sixth value
+  std::fprintf(f, "%f\n%f\n%f\n%d\n%d\n%f\n", prm->tblend, prm->pin, prm->nu, prm->d1, prm->delta,
+               prm->blend);
+  std::fclose(f);
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_pipe_m_mask(int lx0, int l0, int d, uint8_t* out) {
+  if (!out || lx0 < 1 || l0 < 1 || d < 0) return fslbm_set_error(FSLBM_ERR_ARG, "pipe_m_mask: bad argument");
+  // pipe.m:38-60. MATLAB indices are 1-based: cell (i,j) of the lx0 x lx0 block is fluid when
+  // (i-o)^2 + (j-o)^2 <= r^2 with o = r = lx0/2; planes 1..d and l-d+1..l mark fluid as 1.
+  const int lx = lx0 + 2 * d, lz = l0 + 2 * d;
+  const double o = lx0 / 2.0;
+  for (int k = 0; k < lz; ++k) {
+    const bool buffer = k < d || k >= lz - d;
+    for (int j = 0; j < lx; ++j)
+      for (int i = 0; i < lx; ++i) {
+        const int ii = i - d + 1, jj = j - d + 1;   // 1-based inside the unpadded block
+        uint8_t v = kWall;
+        if (ii >= 1 && ii <= lx0 && jj >= 1 && jj <= lx0 &&
+            (ii - o) * (ii - o) + (jj - o) * (jj - o) <= o * o)
+          v = buffer ? kBuf : 0;
+        out[size_t(i) + size_t(lx) * (j + size_t(lx) * k)] = v;
+      }
+  }
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_ref_mask_to_core(const uint8_t* m, int lx, int ly, int lz_ref, int d2,
+                                      uint8_t* core) {
+  if (!m || !core || lx < 3 || ly < 3 || d2 < 1 || lz_ref <= 2 * d2)
+    return fslbm_set_error(FSLBM_ERR_ARG, "ref_mask_to_core: bad argument");
+  const size_t plane = size_t(lx) * ly;
+  const int L = lz_ref - 2 * d2;
+  if (L < d2)
+    return fslbm_set_error(FSLBM_ERR_ARG, "ref_mask_to_core: %d fluid planes shorter than the buffer depth %d", L, d2);
+  for (size_t j = 0; j < plane; ++j) {
+    const uint8_t v = m[plane * d2 + j];
+    if (v != 0 && v != kWall)
+      return fslbm_set_error(FSLBM_ERR_ARG, "ref_mask_to_core: value %d in the first fluid plane", int(v));
+    const int x = int(j % lx), y = int(j / lx);
+    if (v == 0 && (x == 0 || y == 0 || x == lx - 1 || y == ly - 1))
+      return fslbm_set_error(FSLBM_ERR_ARG, "ref_mask_to_core: fluid cell (%d,%d) on the box rim", x, y);
+    core[j] = v;
+  }
+  for (int z = 0; z < lz_ref; ++z) {
+    const bool buffer = z < d2 || z >= lz_ref - d2;
+    for (size_t j = 0; j < plane; ++j) {
+      const uint8_t v = m[plane * z + j];
+      const uint8_t want = core[j] == kWall ? kWall : (buffer ? kBuf : uint8_t(0));
+      if (v != want)
+        return fslbm_set_error(FSLBM_ERR_ARG,
+                               "ref_mask_to_core: plane %d cell %zu is %d, expected %d (the periodic core "
+                               "needs identical planes and buffers that copy them)",
+                               z, j, int(v), int(want));
+    }
+  }
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_init_poiseuille(const fslbm_domain* dom, double umax, double noise, int modes,
+                                     double mode_amp, uint64_t seed, double* p, double* u, double* v,
+                                     double* w) {
+  if (!dom || !p || !u || !v || !w || dom->lx < 1 || dom->ly < 1 || dom->lz < 1 || modes < 0)
+    return fslbm_set_error(FSLBM_ERR_ARG, "init_poiseuille: bad argument");
+  const int lx = dom->lx, ly = dom->ly, L = dom->lz;
+  const size_t plane = size_t(lx) * ly;
+  std::vector<uint8_t> fluid(plane);
+  double R = dom->radius, cx = dom->cx, cy = dom->cy;
+  size_t nf = 0;
+  double sx = 0, sy = 0;
+  for (size_t j = 0; j < plane; ++j) {
+    const int x = int(j % lx), y = int(j / lx);
+    bool f;
+    if (dom->mask) f = dom->mask[j] == 0;
+    else f = (x - cx) * (x - cx) + (y - cy) * (y - cy) <= R * R;
+    fluid[j] = f;
+    if (f) { ++nf; sx += x; sy += y; }
+  }
+  if (!nf) return fslbm_set_error(FSLBM_ERR_ARG, "init_poiseuille: no fluid cells");
+  if (dom->mask || R <= 0) {
+    cx = sx / double(nf); cy = sy / double(nf);
+    double r2max = 0;
+    for (size_t j = 0; j < plane; ++j)
+      if (fluid[j]) {
+        const double dx = int(j % lx) - cx, dy = int(j / lx) - cy;
+        r2max = std::fmax(r2max, dx * dx + dy * dy);
+      }
+    R = std::sqrt(r2max) + 0.5;
+  }
+  // random phases of the perturbation modes
+  std::vector<double> ph(4 * size_t(modes));
+  for (int m = 0; m < modes; ++m)
+    for (int k = 0; k < 4; ++k) ph[4 * m + k] = M_PI * (1.0 + unit_pm(seed ^ 0xA5A5A5A5ull, 4ull * m + k));
+  for (int z = 0; z < L; ++z)
+    for (size_t j = 0; j < plane; ++j) {
+      const size_t idx = size_t(z) * plane + j;
+      if (!fluid[j]) { p[idx] = u[idx] = v[idx] = w[idx] = 0.0; continue; }
+      const double dx = int(j % lx) - cx, dy = int(j / lx) - cy;
+      const double s2 = (dx * dx + dy * dy) / (R * R), s = std::sqrt(s2);
+      const double th = std::atan2(dy, dx);
+      double du = noise * umax * unit_pm(seed, 4 * idx + 1);
+      double dv = noise * umax * unit_pm(seed, 4 * idx + 2);
+      double dw = noise * umax * unit_pm(seed, 4 * idx + 3);
+      const double env = 2.6 * s * (1.0 - std::fmin(s2, 1.0));
+      for (int m = 0; m < modes; ++m) {
+        const double kz = 2.0 * M_PI * double(m + 1) * z / double(L);
+        const int n = 1 + m % 4;
+        dw += mode_amp * umax * env * std::sin(kz + ph[4 * m]) * std::cos(n * th + ph[4 * m + 1]);
+        du += mode_amp * umax * env * std::cos(kz + ph[4 * m + 2]) * std::sin(n * th + ph[4 * m + 3]);
+        dv += mode_amp * umax * env * std::sin(kz + ph[4 * m + 2]) * std::cos(n * th + ph[4 * m + 3]);
+      }
+      p[idx] = 0.0;
+      u[idx] = du;
+      v[idx] = dv;
+      w[idx] = -umax * std::fmax(0.0, 1.0 - s2) + dw;   // stored velocity is the negated physical one
+    }
+  return FSLBM_OK;
+}

@@ -1,0 +1,80 @@
+// Internal declarations shared by the host runtime and the kernel launchers.
+#pragma once
+#include <cstdint>
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include "../../include/fslbm.h"
+#include "common.h"
+
+namespace fslbm {
+
+struct StepGeom;
+
+// Device-side counters of a solve: steps done and monitor records written.
+struct DevCounters {
+  long long steps;
+  long long records;
+};
+
+struct StepLaunch {
+  int dtype;                 // fslbm_dtype of the storage
+  int d1;
+  const CUtensorMap* map;    // input state tensor map (host copy; passed by value)
+  int lxp, ly, L;
+  int ntiles, chunk, nchunks;
+  const int2* tiles;
+  const uint8_t* mask;
+  const void* colcoef;
+  void* out;
+  const double* gauge;
+  unsigned* err;
+  DevCounters* counters;     // steps incremented by the launch
+  // constants in double; converted to the compute type by the launcher
+  double tb, cc, pin, dtddy, m, c0, c1, c2, fx, fy, fz;
+};
+
+size_t step_smem_bytes(int dtype, int d1);
+bool step_supported(int dtype, int d1);
+cudaError_t step_prepare(int dtype, int d1);   // sets the dynamic shared memory attribute
+cudaError_t launch_step(const StepLaunch& a, cudaStream_t st);
+
+struct MonitorLaunch {
+  int dtype;
+  const void* state;
+  const uint8_t* mask;
+  int lxp, lx, ly, L;
+  double pin, nu, radius, l1;
+  int sx, sy, sz;             // sample cell
+  fslbm_monitor* log;
+  int log_cap;
+  double* gauge_out;
+  DevCounters* counters;
+};
+cudaError_t launch_monitor(const MonitorLaunch& a, cudaStream_t st);
+
+cudaError_t launch_zero_walls(int dtype, void* state, const uint8_t* mask, int lxp, int ly, int L,
+                              cudaStream_t st);
+cudaError_t launch_plane_stats(int dtype, const void* state, const uint8_t* mask, int lxp, int ly,
+                               int L, int d2, int xs, double pin, int cnt, int do_mean,
+                               int do_fluct, double* acc, cudaStream_t st);
+cudaError_t launch_profile(int dtype, const void* state, int lxp, int ly, int L, double* acc,
+                           cudaStream_t st);
+cudaError_t launch_check(int dtype, const void* state, size_t n_per_field, double* out,
+                         cudaStream_t st);
+// Converts between the storage type and FP32/FP64 staging buffers (dense per field, pitched).
+// src/dst: dense [4][L][ly][lx] staging arrays; state: pitched [4][L][ly][lxp].
+cudaError_t launch_convert_in(int dtype, void* state, const void* src, int src_is_f64, int lx,
+                              int lxp, int ly, int L, cudaStream_t st);
+cudaError_t launch_convert_out(int dtype, const void* state, void* dst, int dst_is_f64, int lx,
+                               int lxp, int ly, int L, cudaStream_t st);
+
+}  // namespace fslbm
+
+namespace fslbm {
+// TMA box of the step kernel for (dtype, d1): slot row length, rows, halos.
+bool step_box(int dtype, int d1, int* sw, int* sh, int* hx, int* hy);
+// Gathers the YZ plane x = idx (kind 0, out [4][L][ly]) or the XY plane z = idx
+// (kind 1, out [4][ly][lx]) of the four fields as FP32 into device memory.
+cudaError_t launch_gather_plane(int dtype, const void* state, int lx, int lxp, int ly, int L,
+                                int kind, int idx, float* out, cudaStream_t st);
+}  // namespace fslbm

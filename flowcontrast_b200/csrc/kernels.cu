@@ -1,0 +1,401 @@
+// Kernel launchers and the small auxiliary kernels of the solve runtime (monitor reduction,
+// statistics accumulation, field conversion, divergence check).
+#include <cstdio>
+#include "internal.h"
+#include "step_kernel.cuh"
+
+namespace fslbm {
+
+// ------------------------------------------------------------------------------------------
+// step dispatch
+// ------------------------------------------------------------------------------------------
+template <class TS, int D1>
+static cudaError_t launch_step_t(const StepLaunch& a, cudaStream_t st) {
+  using TC = typename Compute<TS>::type;
+  using Tl = StepTile<TS, D1>;
+  StepGeom g;
+  g.lxp = a.lxp; g.ly = a.ly; g.L = a.L;
+  g.ntiles = a.ntiles; g.chunk = a.chunk;
+  g.tiles = a.tiles; g.mask = a.mask; g.colcoef = a.colcoef; g.out = a.out;
+  g.gauge = a.gauge; g.err = a.err;
+  g.step_counter = a.counters ? &a.counters->steps : nullptr;
+  StepConst<TC> k;
+  k.tb = TC(a.tb); k.cc = TC(a.cc); k.pin = TC(a.pin); k.dtddy = TC(a.dtddy); k.m = TC(a.m);
+  k.c0 = TC(a.c0); k.c1 = TC(a.c1); k.c2 = TC(a.c2);
+  k.fx = TC(a.fx); k.fy = TC(a.fy); k.fz = TC(a.fz);
+  const int grid = a.ntiles * a.nchunks;
+  fslbm_step_kernel<TS, D1><<<grid, kThreads, Tl::SMEM_BYTES, st>>>(*a.map, g, k);
+  return cudaGetLastError();
+}
+
+template <class TS, int D1>
+static cudaError_t prepare_t() {
+  using Tl = StepTile<TS, D1>;
+  return cudaFuncSetAttribute(fslbm_step_kernel<TS, D1>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, int(Tl::SMEM_BYTES));
+}
+
+template <class TS, int D1> static size_t smem_t() { return StepTile<TS, D1>::SMEM_BYTES; }
+
+bool step_supported(int dtype, int d1) {
+  if (dtype == FSLBM_F32) return d1 >= 1 && d1 <= 3;
+  if (dtype == FSLBM_F64) return d1 >= 1 && d1 <= 2;
+  return false;
+}
+
+size_t step_smem_bytes(int dtype, int d1) {
+  if (dtype == FSLBM_F32) {
+    if (d1 == 1) return smem_t<float, 1>();
+    if (d1 == 2) return smem_t<float, 2>();
+    if (d1 == 3) return smem_t<float, 3>();
+  } else if (dtype == FSLBM_F64) {
+    if (d1 == 1) return smem_t<double, 1>();
+    if (d1 == 2) return smem_t<double, 2>();
+  }
+  return 0;
+}
+
+cudaError_t step_prepare(int dtype, int d1) {
+  if (dtype == FSLBM_F32) {
+    if (d1 == 1) return prepare_t<float, 1>();
+    if (d1 == 2) return prepare_t<float, 2>();
+    if (d1 == 3) return prepare_t<float, 3>();
+  } else if (dtype == FSLBM_F64) {
+    if (d1 == 1) return prepare_t<double, 1>();
+    if (d1 == 2) return prepare_t<double, 2>();
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_step(const StepLaunch& a, cudaStream_t st) {
+  if (a.dtype == FSLBM_F32) {
+    if (a.d1 == 1) return launch_step_t<float, 1>(a, st);
+    if (a.d1 == 2) return launch_step_t<float, 2>(a, st);
+    if (a.d1 == 3) return launch_step_t<float, 3>(a, st);
+  } else if (a.dtype == FSLBM_F64) {
+    if (a.d1 == 1) return launch_step_t<double, 1>(a, st);
+    if (a.d1 == 2) return launch_step_t<double, 2>(a, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// ------------------------------------------------------------------------------------------
+// block reduction helper (FP64)
+// ------------------------------------------------------------------------------------------
+template <int NV>
+__device__ void block_sum(double (&v)[NV], double* sh /* NV * 32 */) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) sh[k * 32 + warp] = v[k];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double s = lane < nw ? sh[k * 32 + lane] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      v[k] = s;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// monitor (FSLBM.cu:632-666), FP64 sums, one block
+// ------------------------------------------------------------------------------------------
+template <class TS>
+__global__ void monitor_kernel(MonitorLaunch a) {
+  __shared__ double sh[3 * 32];
+  const TS* st = reinterpret_cast<const TS*>(a.state);
+  const size_t FS = size_t(a.lxp) * a.ly * a.L;
+  const TS pin = TS(a.pin);
+  double v[3] = {0, 0, 0};   // sum w, sum p, sum (p - pin) over non-wall cells of plane z=0
+  for (int j = threadIdx.x; j < a.lxp * a.ly; j += blockDim.x) {
+    const TS p = st[j];
+    v[0] += double(st[3 * FS + j]);
+    v[1] += double(p);
+    if (a.mask[j] != kWall) v[2] += double(TS(p - pin));   // the outlet buffer copy's p
+  }
+  block_sum<3>(v, sh);
+  if (threadIdx.x == 0) {
+    const double q1 = v[0] / a.l1, p1 = v[1] / a.l1, p2 = v[2] / a.l1;
+    fslbm_monitor r;
+    r.step = a.counters->steps;
+    r.q1 = q1; r.q2 = q1; r.p1 = p1; r.p2 = p2;
+    r.f = (p1 - p2) / q1 / q1 / 3.0 * 4.0 * a.radius / double(a.L);
+    r.sample = double(st[3 * FS + (size_t(a.sz) * a.ly + a.sy) * a.lxp + a.sx]);
+    r.re = 2.0 * a.radius * q1 / a.nu;
+    const long long idx = a.counters->records;
+    a.log[idx % a.log_cap] = r;
+    a.counters->records = idx + 1;
+    *a.gauge_out = p2;
+  }
+}
+
+cudaError_t launch_monitor(const MonitorLaunch& a, cudaStream_t st) {
+  if (a.dtype == FSLBM_F32) monitor_kernel<float><<<1, 512, 0, st>>>(a);
+  else if (a.dtype == FSLBM_F64) monitor_kernel<double><<<1, 512, 0, st>>>(a);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------
+// wall zeroing, conversion, check
+// ------------------------------------------------------------------------------------------
+template <class TS>
+__global__ void zero_walls_kernel(TS* s, const uint8_t* mask, int lxp, int ly, int L) {
+  const size_t FS = size_t(lxp) * ly * L;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < FS;
+       i += size_t(gridDim.x) * blockDim.x) {
+    if (mask[i % (size_t(lxp) * ly)] == kWall) {
+      s[i] = TS(0); s[FS + i] = TS(0); s[2 * FS + i] = TS(0); s[3 * FS + i] = TS(0);
+    }
+  }
+}
+
+cudaError_t launch_zero_walls(int dtype, void* state, const uint8_t* mask, int lxp, int ly, int L,
+                              cudaStream_t st) {
+  const int grid = 592;
+  if (dtype == FSLBM_F32)
+    zero_walls_kernel<float><<<grid, 256, 0, st>>>(reinterpret_cast<float*>(state), mask, lxp, ly, L);
+  else if (dtype == FSLBM_F64)
+    zero_walls_kernel<double><<<grid, 256, 0, st>>>(reinterpret_cast<double*>(state), mask, lxp, ly, L);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+template <class TS, class TH>
+__global__ void convert_in_kernel(TS* s, const TH* src, int lx, int lxp, int ly, int L) {
+  const size_t n = size_t(lx) * ly * L, FS = size_t(lxp) * ly * L;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < 4 * n;
+       i += size_t(gridDim.x) * blockDim.x) {
+    const size_t f = i / n, r = i % n, x = r % lx, yz = r / lx;
+    s[f * FS + yz * lxp + x] = TS(src[i]);
+  }
+}
+template <class TS, class TH>
+__global__ void convert_out_kernel(const TS* s, TH* dst, int lx, int lxp, int ly, int L) {
+  const size_t n = size_t(lx) * ly * L, FS = size_t(lxp) * ly * L;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < 4 * n;
+       i += size_t(gridDim.x) * blockDim.x) {
+    const size_t f = i / n, r = i % n, x = r % lx, yz = r / lx;
+    dst[i] = TH(s[f * FS + yz * lxp + x]);
+  }
+}
+
+cudaError_t launch_convert_in(int dtype, void* state, const void* src, int src_is_f64, int lx,
+                              int lxp, int ly, int L, cudaStream_t st) {
+  const int grid = 1184;
+  if (dtype == FSLBM_F32) {
+    if (src_is_f64) convert_in_kernel<float, double><<<grid, 256, 0, st>>>((float*)state, (const double*)src, lx, lxp, ly, L);
+    else convert_in_kernel<float, float><<<grid, 256, 0, st>>>((float*)state, (const float*)src, lx, lxp, ly, L);
+  } else if (dtype == FSLBM_F64) {
+    if (src_is_f64) convert_in_kernel<double, double><<<grid, 256, 0, st>>>((double*)state, (const double*)src, lx, lxp, ly, L);
+    else convert_in_kernel<double, float><<<grid, 256, 0, st>>>((double*)state, (const float*)src, lx, lxp, ly, L);
+  } else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_convert_out(int dtype, const void* state, void* dst, int dst_is_f64, int lx,
+                               int lxp, int ly, int L, cudaStream_t st) {
+  const int grid = 1184;
+  if (dtype == FSLBM_F32) {
+    if (dst_is_f64) convert_out_kernel<float, double><<<grid, 256, 0, st>>>((const float*)state, (double*)dst, lx, lxp, ly, L);
+    else convert_out_kernel<float, float><<<grid, 256, 0, st>>>((const float*)state, (float*)dst, lx, lxp, ly, L);
+  } else if (dtype == FSLBM_F64) {
+    if (dst_is_f64) convert_out_kernel<double, double><<<grid, 256, 0, st>>>((const double*)state, (double*)dst, lx, lxp, ly, L);
+    else convert_out_kernel<double, float><<<grid, 256, 0, st>>>((const double*)state, (float*)dst, lx, lxp, ly, L);
+  } else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+// out[0] = number of non-finite values, out[1] = max |u|,|v|,|w| (FP64)
+template <class TS>
+__global__ void check_kernel(const TS* s, size_t n, double* out) {
+  __shared__ double sh[2 * 32];
+  double v[2] = {0, 0};
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < 4 * n;
+       i += size_t(gridDim.x) * blockDim.x) {
+    const double a = double(s[i]);
+    if (!isfinite(a)) v[0] += 1.0;
+    else if (i >= n) v[1] = fmax(v[1], fabs(a));
+  }
+  // max via a separate warp pass: reuse block_sum for the count, max by shuffles
+  double m = v[1];
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  double c[1] = {v[0]};
+  block_sum<1>(c, sh);
+  __shared__ double shm[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) shm[warp] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mm = 0;
+    for (int k = 0; k < int((blockDim.x + 31) >> 5); ++k) mm = fmax(mm, shm[k]);
+    atomicAdd(&out[0], c[0]);
+    unsigned long long* mp = reinterpret_cast<unsigned long long*>(&out[1]);
+    unsigned long long old = *mp;
+    while (__longlong_as_double(old) < mm) {
+      const unsigned long long prev = atomicCAS(mp, old, __double_as_longlong(mm));
+      if (prev == old) break;
+      old = prev;
+    }
+  }
+}
+
+cudaError_t launch_check(int dtype, const void* state, size_t n_per_field, double* out,
+                         cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(out, 0, 2 * sizeof(double), st);
+  if (e) return e;
+  if (dtype == FSLBM_F32) check_kernel<float><<<296, 256, 0, st>>>((const float*)state, n_per_field, out);
+  else if (dtype == FSLBM_F64) check_kernel<double><<<296, 256, 0, st>>>((const double*)state, n_per_field, out);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------
+// reference plane statistics (FSLBM.cu:715-748) on the YZ plane x = xs of the reference
+// layout: rows y, columns z_ref in [0, L+2*d2); buffer planes are the wrapped core planes with
+// p +- pin on non-wall cells, in the storage type's arithmetic as the reference's bcond does.
+// acc: 11 arrays of ly*(L+2*d2) doubles; cnt is the mean count including this sample.
+// ------------------------------------------------------------------------------------------
+template <class TS>
+__global__ void plane_stats_kernel(const TS* s, const uint8_t* mask, int lxp, int ly, int L,
+                                   int d2, int xs, double pin_d, int cnt, double* acc) {
+  const int Lr = L + 2 * d2;
+  const size_t n = size_t(ly) * Lr, FS = size_t(lxp) * ly * L;
+  const TS pin = TS(pin_d);
+  for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n;
+       k += size_t(gridDim.x) * blockDim.x) {
+    const int y = int(k % ly), zr = int(k / ly);
+    int zc = zr - d2, jump = 0;
+    if (zc < 0) { zc += L; jump = 1; } else if (zc >= L) { zc -= L; jump = -1; }
+    const size_t o = (size_t(zc) * ly + y) * lxp + xs;
+    TS p = s[o];
+    if (mask[size_t(y) * lxp + xs] != kWall) {
+      if (jump == 1) p = TS(p + pin);
+      else if (jump == -1) p = TS(p - pin);
+    }
+    const double qp = double(p), qu = double(s[FS + o]), qv = double(s[2 * FS + o]),
+                 qw = double(s[3 * FS + o]);
+    const double c = double(cnt);
+    double* a = acc;
+    a[k] += qp;          const double dd1 = a[k] / c - qp;
+    a[n + k] += qu;      const double dd2 = a[n + k] / c - qu;
+    a[2 * n + k] += qv;  const double dd3 = a[2 * n + k] / c - qv;
+    a[3 * n + k] += qw;  const double dd4 = a[3 * n + k] / c - qw;
+    a[4 * n + k] += fabs(dd1);
+    a[5 * n + k] += fabs(dd2);
+    a[6 * n + k] += fabs(dd3);
+    a[7 * n + k] += fabs(dd4);
+    a[8 * n + k] += dd2 * dd3;
+    a[9 * n + k] += dd2 * dd4;
+    a[10 * n + k] += dd4 * dd3;
+  }
+}
+
+cudaError_t launch_plane_stats(int dtype, const void* state, const uint8_t* mask, int lxp, int ly,
+                               int L, int d2, int xs, double pin, int cnt, int, int, double* acc,
+                               cudaStream_t st) {
+  const int grid = 148;
+  if (dtype == FSLBM_F32)
+    plane_stats_kernel<float><<<grid, 256, 0, st>>>((const float*)state, mask, lxp, ly, L, d2, xs, pin, cnt, acc);
+  else if (dtype == FSLBM_F64)
+    plane_stats_kernel<double><<<grid, 256, 0, st>>>((const double*)state, mask, lxp, ly, L, d2, xs, pin, cnt, acc);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------
+// full-volume profile statistics: per column (x,y), sums over z of
+// p,u,v,w,uu,vv,ww,uv,uw,vw (FP64). Block = 32 columns x 8 z-lanes; atomics per block.
+// ------------------------------------------------------------------------------------------
+template <class TS>
+__global__ void profile_kernel(const TS* s, int lxp, int ly, int L, double* acc) {
+  __shared__ double sh[10][8][33];
+  const int tx = threadIdx.x & 31, tz = threadIdx.x >> 5;
+  const int x = blockIdx.x * 32 + tx, y = blockIdx.y;
+  const size_t FS = size_t(lxp) * ly * L, cs = size_t(lxp) * ly;
+  double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (x < lxp) {
+    for (int z = blockIdx.z * 8 + tz; z < L; z += gridDim.z * 8) {
+      const size_t o = (size_t(z) * ly + y) * lxp + x;
+      const double p = s[o], u = s[FS + o], vv = s[2 * FS + o], w = s[3 * FS + o];
+      v[0] += p; v[1] += u; v[2] += vv; v[3] += w;
+      v[4] += u * u; v[5] += vv * vv; v[6] += w * w; v[7] += u * vv; v[8] += u * w; v[9] += vv * w;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 10; ++k) sh[k][tz][tx] = v[k];
+  __syncthreads();
+  if (tz == 0 && x < lxp) {
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+      double t = 0;
+      for (int j = 0; j < 8; ++j) t += sh[k][j][tx];
+      atomicAdd(&acc[k * cs + size_t(y) * lxp + x], t);
+    }
+  }
+}
+
+cudaError_t launch_profile(int dtype, const void* state, int lxp, int ly, int L, double* acc,
+                           cudaStream_t st) {
+  dim3 grid((lxp + 31) / 32, ly, (L + 63) / 64 < 8 ? (L + 63) / 64 : 8);
+  if (grid.z < 1) grid.z = 1;
+  if (dtype == FSLBM_F32) profile_kernel<float><<<grid, 256, 0, st>>>((const float*)state, lxp, ly, L, acc);
+  else if (dtype == FSLBM_F64) profile_kernel<double><<<grid, 256, 0, st>>>((const double*)state, lxp, ly, L, acc);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+}  // namespace fslbm
+
+namespace fslbm {
+
+bool step_box(int dtype, int d1, int* sw, int* sh, int* hx, int* hy) {
+#define FSLBM_BOX(T, D)                                                              \
+  do {                                                                               \
+    using Tl = StepTile<T, D>;                                                       \
+    *sw = Tl::SW; *sh = Tl::SH; *hx = Tl::HX; *hy = Tl::HY;                          \
+    return true;                                                                     \
+  } while (0)
+  if (dtype == FSLBM_F32) {
+    if (d1 == 1) FSLBM_BOX(float, 1);
+    if (d1 == 2) FSLBM_BOX(float, 2);
+    if (d1 == 3) FSLBM_BOX(float, 3);
+  } else if (dtype == FSLBM_F64) {
+    if (d1 == 1) FSLBM_BOX(double, 1);
+    if (d1 == 2) FSLBM_BOX(double, 2);
+  }
+#undef FSLBM_BOX
+  return false;
+}
+
+template <class TS>
+__global__ void gather_plane_kernel(const TS* s, int lx, int lxp, int ly, int L, int kind, int idx,
+                                    float* out) {
+  const size_t FS = size_t(lxp) * ly * L;
+  const size_t n = kind == 0 ? size_t(L) * ly : size_t(ly) * lx;
+  for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < 4 * n;
+       k += size_t(gridDim.x) * blockDim.x) {
+    const size_t f = k / n, r = k % n;
+    size_t o;
+    if (kind == 0) o = (r / ly * ly + r % ly) * lxp + idx;          // r = y + ly*z
+    else o = (size_t(idx) * ly + r / lx) * lxp + r % lx;            // r = x + lx*y
+    out[k] = float(s[f * FS + o]);
+  }
+}
+
+cudaError_t launch_gather_plane(int dtype, const void* state, int lx, int lxp, int ly, int L,
+                                int kind, int idx, float* out, cudaStream_t st) {
+  if (dtype == FSLBM_F32)
+    gather_plane_kernel<float><<<148, 256, 0, st>>>((const float*)state, lx, lxp, ly, L, kind, idx, out);
+  else if (dtype == FSLBM_F64)
+    gather_plane_kernel<double><<<148, 256, 0, st>>>((const double*)state, lx, lxp, ly, L, kind, idx, out);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+}  // namespace fslbm

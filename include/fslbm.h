@@ -1,0 +1,206 @@
+/* fslbm.h -- C ABI of the B200 fractional-step lattice Boltzmann (FSLBM) pipe solver.
+ *
+ * The reference (alparmat/FlowContrast) has no library API: its drop-in surface is the
+ * executable PipeDemoStandalone/FSLBM.cu plus the files it reads and writes in the working
+ * directory. Each entry point below names the reference code it replaces (file:line in
+ * PipeDemoStandalone/FSLBM.cu or pipe.m). The drop-in executable `fslbm_pipe` and the Python
+ * package are both built on this ABI.
+ *
+ * Conventions
+ *  - Every function returns 0 (FSLBM_OK) or a negative FSLBM_ERR_* code; the message of the last
+ *    error on the calling thread is read with fslbm_last_error().
+ *  - Axes follow the reference: x and y span the pipe cross-section (x fastest in memory), z is
+ *    streamwise (slowest). Host arrays are dense lx*ly*lz, index x + lx*(y + ly*z).
+ *  - p is the density deviation (rho - 1) of the incompressible He-Luo equilibrium; u, v, w are
+ *    the stored velocity components, which are the NEGATED physical velocity (FSLBM.cu:137-173
+ *    pulls f at x+c and accumulates +c). Dumps keep this sign, as the reference's viewers expect.
+ *  - Threading: a context and its solves may be used from one host thread at a time. The
+ *    server (fslbm_server_*) runs its own worker thread and its calls are thread-safe.
+ */
+#ifndef FSLBM_H
+#define FSLBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FSLBM_OK 0
+#define FSLBM_ERR_ARG (-1)      /* invalid argument, size or geometry */
+#define FSLBM_ERR_CUDA (-2)     /* a CUDA call failed */
+#define FSLBM_ERR_STATE (-3)    /* call out of order (e.g. no fields set) */
+#define FSLBM_ERR_IO (-4)       /* file missing, truncated or malformed */
+#define FSLBM_ERR_DIVERGED (-5) /* non-finite values found by the divergence check */
+#define FSLBM_ERR_TIMEOUT (-6)  /* a bounded device-side wait gave up */
+#define FSLBM_ERR_BUDGET (-7)   /* request larger than the server's memory budget */
+#define FSLBM_ERR_NOTFOUND (-8) /* unknown request id */
+
+typedef enum {
+  FSLBM_F64 = 0, /* FP64 storage and arithmetic */
+  FSLBM_F32 = 1, /* FP32 storage and arithmetic (the reference's precision) */
+  FSLBM_F16 = 2  /* mixed: FP16 storage of scaled deviations, FP32 arithmetic */
+} fslbm_dtype;
+
+typedef struct fslbm_ctx fslbm_ctx;
+typedef struct fslbm_solve fslbm_solve;
+typedef struct fslbm_batch fslbm_batch;
+typedef struct fslbm_server fslbm_server;
+
+/* Periodic pipe domain. Replaces the hard-coded dims of FSLBM.cu:512-514 and the mask read of
+ * FSLBM.cu:478-485. The streamwise direction is periodic with a pressure jump `pin` across the
+ * seam, which is what the reference's buffer planes and bcond copies implement
+ * (FSLBM.cu:291-301); lz counts the fluid planes only (the reference's lz - 2*d2). */
+typedef struct {
+  int lx, ly;            /* cross-section size in cells */
+  int lz;                /* streamwise period in cells */
+  const uint8_t* mask;   /* lx*ly cross-section: 0 fluid, 125 wall; NULL selects the circle */
+  double radius;         /* circle radius; also the r of the friction factor and Re (FSLBM.cu:650,660) */
+  double cx, cy;         /* circle centre: fluid iff (x-cx)^2 + (y-cy)^2 <= radius^2 */
+  int buffer_depth;      /* d2 of the reference layout used by plane dumps and statistics */
+} fslbm_domain;
+
+/* Run parameters: the six lines of param.txt (FSLBM.cu:502-507) plus additions. */
+typedef struct {
+  double tblend;        /* time-step blend b (FSLBM.cu:269) */
+  double pin;           /* pressure jump across the periodic seam (FSLBM.cu:296,300) */
+  double nu;            /* target viscosity; dtddy = nu - 0.16666666 (FSLBM.cu:599) */
+  int d1;               /* coarse corrective stride (FSLBM.cu:243-253); 1..3 */
+  int delta;            /* statistics reset policy (FSLBM.cu:683-690) */
+  double blend;         /* corrector order blend, 0: order 2, 1: order 4 (FSLBM.cu:231) */
+  int monitor_every;    /* monitor + pressure gauge period; 50 in the reference (FSLBM.cu:630) */
+  double force[3];      /* addition: body force per step on (u,v,w), stored-velocity sign */
+} fslbm_params;
+
+/* One monitor record (FSLBM.cu:632-666): means over the first fluid plane (q1, p1) and over the
+ * first outlet buffer plane (q2, p2) per fluid cell, friction factor f, the w sample at the box
+ * centre and Re = 2 r q1 / nu. Reductions are FP64. */
+typedef struct {
+  int64_t step;
+  double q1, q2, p1, p2, f, sample, re;
+} fslbm_monitor;
+
+typedef struct {
+  int64_t cells;         /* lx*ly*lz */
+  int64_t fluid_cells;   /* non-wall cells */
+  int64_t bytes_device;  /* device memory held by the solve */
+  int64_t steps;         /* steps advanced so far */
+  int lx_pitch;          /* padded row length in device memory */
+  int dtype;
+  double last_step_ms;   /* device time of the last fslbm_solve_step call */
+  int64_t kernel_launches; /* kernels this solve has launched (steps, monitors, statistics) */
+} fslbm_info;
+
+/* ---- errors and version ---- */
+const char* fslbm_version(void);
+/* Copies the calling thread's last error message into buf; returns its code. */
+int fslbm_last_error(char* buf, size_t n);
+
+/* ---- context: one device, one stream (replaces cudaSetDevice(0), FSLBM.cu:490) ---- */
+int fslbm_ctx_create(int device, fslbm_ctx** out);
+int fslbm_ctx_destroy(fslbm_ctx* ctx);
+
+/* ---- solve (replaces main's set-up and time loop, FSLBM.cu:489-905) ---- */
+int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const fslbm_params* prm,
+                       fslbm_dtype dtype, fslbm_solve** out);
+int fslbm_solve_destroy(fslbm_solve* s);
+/* Live parameter update, as the reference's re-read of param.txt every 500 steps
+ * (FSLBM.cu:669-677). d1 may change only to another supported stride. */
+int fslbm_solve_set_params(fslbm_solve* s, const fslbm_params* prm);
+/* Host fields in, lx*ly*lz each, FP64 (host_dtype FSLBM_F64) or FP32 (FSLBM_F32). Wall cells
+ * are set to zero, the invariant the reference's bcond restores every step (FSLBM.cu:290).
+ * Replaces the restart loader initphys1 (FSLBM.cu:386-418). */
+int fslbm_solve_set_fields(fslbm_solve* s, fslbm_dtype host_dtype, const void* p, const void* u,
+                           const void* v, const void* w);
+int fslbm_solve_get_fields(fslbm_solve* s, fslbm_dtype host_dtype, void* p, void* u, void* v,
+                           void* w);
+/* Advances nsteps time steps, asynchronously on the context's stream. Each step is one fused
+ * kernel (predictor, corrector, periodic pressure-jump and wall boundaries, gauge). Every
+ * monitor_every steps a monitor record is produced on the device and its p2 gauges the next
+ * step (FSLBM.cu:628, 637-647). Replaces FSLBM.cu:620-628 (about 350 launches per step). */
+int fslbm_solve_step(fslbm_solve* s, int64_t nsteps);
+int fslbm_solve_sync(fslbm_solve* s);
+/* Latest monitor record (synchronises). Returns FSLBM_ERR_STATE if none exists yet. */
+int fslbm_solve_monitor(fslbm_solve* s, fslbm_monitor* out);
+/* Drains up to `max` monitor records produced since the last drain, oldest first. */
+int fslbm_solve_monitor_log(fslbm_solve* s, fslbm_monitor* out, int max, int* n_out);
+/* Non-finite scan of the current fields (FP64 reduction); FSLBM_ERR_DIVERGED if any. */
+int fslbm_solve_check(fslbm_solve* s, double* max_abs_u);
+int fslbm_solve_info(fslbm_solve* s, fslbm_info* out);
+/* Per-launch device timing of the step kernel: with enable != 0 every step launch is
+ * bracketed by CUDA events on the launching stream. fslbm_solve_kernel_time synchronises and
+ * returns the summed step-kernel time and launch count since the previous call. */
+int fslbm_solve_set_timing(fslbm_solve* s, int enable);
+int fslbm_solve_kernel_time(fslbm_solve* s, double* ms_total, int64_t* launches);
+/* Device pointers of the current state (p, u, v, w in the solve's storage type, row pitch
+ * info.lx_pitch). Valid until the next step, set_fields or destroy. */
+int fslbm_solve_device_fields(fslbm_solve* s, void** p, void** u, void** v, void** w);
+
+/* ---- reference-layout fields: the core plus d2 buffer planes at each streamwise end,
+ *      reconstructed as the bcond copies with the +-pin jump (FSLBM.cu:291-301) ---- */
+/* Host arrays lx*ly*(lz+2*d2) FP32, the reference's restart layout (p3Dii etc., FSLBM.cu:830-856). */
+int fslbm_solve_get_fields_ref(fslbm_solve* s, float* p, float* u, float* v, float* w);
+/* Loads reference-layout fields, keeping planes d2..d2+lz-1 (FSLBM.cu:386-418). */
+int fslbm_solve_set_fields_ref(fslbm_solve* s, const float* p, const float* u, const float* v,
+                               const float* w);
+/* One plane of the reference layout. kind 0: YZ plane x=lx/2, values y + ly*z_ref
+ * (FSLBM.cu:315-324, 784-798); kind 1: XY plane z_ref = lz_ref/2, values x + lx*y
+ * (FSLBM.cu:327-336, 800-814). comp 0..3 = p,u,v,w. */
+int fslbm_solve_get_plane(fslbm_solve* s, int kind, int comp, float* out);
+
+/* ---- statistics ---- */
+/* Reference plane statistics (FSLBM.cu:683-768) on the YZ plane x=lx/2 of the reference layout,
+ * accumulated on the device in FP64. fslbm_stats_sample applies the `delta` reset policy of the
+ * current parameters, then adds one sample (cnt and cnt2 are incremented first, as in the
+ * reference). Outputs are 11 arrays of ly*(lz+2*d2) doubles in the order
+ * _p,_ux,_uy,_uz (sums / cnt), _p2,_ux2,_uy2,_uz2,_uxy2,_uxz2,_uyz2 (sums / cnt2). */
+int fslbm_stats_sample(fslbm_solve* s);
+int fslbm_stats_get(fslbm_solve* s, double* out, int* cnt, int* cnt2);
+/* Restores averaged statistics (the `_*ii.txt` / `_avii.txt` restart, FSLBM.cu:429-468):
+ * the means are multiplied back by their counts. */
+int fslbm_stats_set(fslbm_solve* s, const double* means, int cnt, int cnt2);
+/* Full-volume profile statistics (addition): per cross-section cell, FP64 sums over z and over
+ * samples of p,u,v,w,uu,vv,ww,uv,uw,vw (10 arrays of lx*ly). */
+int fslbm_profile_sample(fslbm_solve* s);
+int fslbm_profile_get(fslbm_solve* s, double* sums, int64_t* nsamples);
+int fslbm_profile_reset(fslbm_solve* s);
+
+/* ---- batched ensemble: many solves advanced by one persistent launch per step group ---- */
+int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, int n, fslbm_batch** out);
+int fslbm_batch_destroy(fslbm_batch* b);
+/* Advances every member nsteps steps; with use_graph the step group is a captured CUDA graph. */
+int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int use_graph);
+int fslbm_batch_sync(fslbm_batch* b);
+
+/* ---- host-side formats and generators ---- */
+/* pipe.txt: one integer per line, x fastest (pipe.m:62). Reads exactly lx*ly*lz values; extra
+ * or missing values are an FSLBM_ERR_IO (the reference's feof loop writes one byte past its
+ * buffer, FSLBM.cu:481-484). */
+int fslbm_read_pipe_txt(const char* path, int lx, int ly, int lz, uint8_t* out);
+int fslbm_write_pipe_txt(const char* path, int lx, int ly, int lz, const uint8_t* mask);
+/* param.txt (FSLBM.cu:502-507): tblend, pin, nu as %e floats, d1 and delta as %d, blend as %e.
+ * Values are rounded to FP32 as the reference reads them. Fields not in the file keep prm's. */
+int fslbm_read_param_txt(const char* path, fslbm_params* prm);
+int fslbm_write_param_txt(const char* path, const fslbm_params* prm);
+/* pipe.m:36-60: circle of diameter lx0 in a (lx0+2d)^2 cross-section, l0 fluid planes between
+ * d buffer planes (value 1) at each end; out holds (lx0+2d)^2 * (l0+2d) bytes. */
+int fslbm_pipe_m_mask(int lx0, int l0, int d, uint8_t* out);
+/* Splits a reference-layout mask (buffer planes included) into the periodic core's
+ * cross-section. Rejects masks the periodic core cannot represent: values other than 0/1/125,
+ * fluid on the box rim or inside the buffers, planes that differ, or buffer planes that are
+ * not the wrapped copies of their source planes. */
+int fslbm_ref_mask_to_core(const uint8_t* mask3d, int lx, int ly, int lz_ref, int d2,
+                           uint8_t* mask2d_out);
+/* Seeded initial fields (addition): Poiseuille w = -umax (1 - r^2/R^2) on the circle plus
+ * uniform noise of amplitude noise*umax on u,v,w (splitmix64 of seed and cell index), and
+ * `modes` random-phase sinusoidal streamwise/azimuthal perturbations of amplitude mode_amp*umax
+ * (0 disables). p = 0. Host arrays of lx*ly*lz doubles. */
+int fslbm_init_poiseuille(const fslbm_domain* dom, double umax, double noise, int modes,
+                          double mode_amp, uint64_t seed, double* p, double* u, double* v,
+                          double* w);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FSLBM_H */

@@ -1,0 +1,37 @@
+"""The CUDA path, driven through the reference-layout entry points of the C ABI
+(fslbm_solve_set_fields_ref / get_fields_ref), against the reference's own kernels' output on
+the golden cases. The periodic core with the +-pin seam must reproduce the reference's buffer
+planes and bcond copies. Tolerance as in test_oracle_golden.py (FP32 against FP32)."""
+import os
+
+import numpy as np
+import pytest
+
+import ref_cases as RC
+from test_oracle_golden import GOLDEN, TOL, load, rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", list(RC.CASES))
+def test_gpu_matches_reference_kernels(built, ctx, name):
+    g = load(name)
+    c = RC.CASES[name]
+    io, ref, prm = RC.inputs(name)
+    keep = RC.nonwall_index(io)
+    core = built.ref_mask_to_core(io, RC.D)
+    lz, ly, lx = io.shape
+    dom = built.make_domain(lx, ly, lz - 2 * RC.D, mask=core, radius=c["lx0"] / 2,
+                            buffer_depth=RC.D)
+    params = built.Params.make(tblend=prm["tblend"], pin=prm["pin"], nu=prm["nu"],
+                               d1=prm["d1"], delta=1, blend=prm["blend"], monitor_every=0)
+    for dt in (built.F32, built.F64):
+        for n in c["steps"]:
+            s = built.Solve(ctx, dom, params, dt)
+            s.set_fields_ref(ref)
+            s.step(n)
+            out = s.get_fields_ref()
+            s.close()
+            got = out.reshape(4, -1)[:, keep].astype(np.float64)
+            ep, eu = rel(got, g[f"step{n}"].astype(np.float64))
+            assert ep < TOL and eu < TOL, (name, dt, n, ep, eu)
