@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -131,6 +132,10 @@ struct fslbm_solve {
   int2* d_tiles = nullptr;
   int ntiles = 0, chunk = 0, nchunks = 0;
   CUtensorMap maps[2];
+  // FP32 column-pair kernel (even d1): tile height, persistent grid, two maps per buffer
+  bool use2 = false;
+  int ty2 = 32, grid2 = 0, packed2 = 1;
+  CUtensorMap maps2p[2], maps2u[2];
   DevCounters* d_counters = nullptr;
   fslbm_monitor* d_log = nullptr;
   int log_cap = 4096;
@@ -189,8 +194,74 @@ static int build_tensor_maps(fslbm_solve* s) {
                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
       return fslbm_set_error(FSLBM_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
+    if (s->use2) {
+      int sw2, ph, uh, hx2, hy2;
+      if (!step2_box(s->prm.d1, s->ty2, &sw2, &ph, &uh, &hx2, &hy2))
+        return fslbm_set_error(FSLBM_ERR_ARG, "no column-pair kernel for d1 %d", s->prm.d1);
+      cuuint32_t boxp[4] = {cuuint32_t(sw2), cuuint32_t(ph), 1, 1};
+      cuuint32_t boxu[4] = {cuuint32_t(sw2), cuuint32_t(uh), 1, 3};
+      r = enc(&s->maps2p[b], dt, 4, s->state[b], dims, strides, boxp, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r == CUDA_SUCCESS)
+        r = enc(&s->maps2u[b], dt, 4, s->state[b], dims, strides, boxu, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS)
+        return fslbm_set_error(FSLBM_ERR_CUDA, "cuTensorMapEncodeTiled (pair kernel) failed (%d)", int(r));
+    }
   }
   return FSLBM_OK;
+}
+
+// Tile list (tiles holding fluid) for a tile of kTX x th cells.
+static std::vector<int2> fluid_tiles(const fslbm_solve* s, int th) {
+  std::vector<int2> tiles;
+  for (int y0 = 0; y0 < s->ly; y0 += th)
+    for (int x0 = 0; x0 < s->lxp; x0 += kTX) {
+      bool any = false;
+      for (int y = y0; y < std::min(y0 + th, s->ly) && !any; ++y)
+        for (int x = x0; x < std::min(x0 + kTX, s->lxp); ++x)
+          if (s->mask[size_t(y) * s->lxp + x] == 0) { any = true; break; }
+      if (any) tiles.push_back(make_int2(x0, y0));
+    }
+  return tiles;
+}
+
+static void choose_chunks(fslbm_solve* s);
+
+// Selects the step kernel for the current dtype and d1, uploads its tile list, builds its
+// tensor maps and sizes its grid. FSLBM_STEP_KERNEL=1 forces the one-column kernel and
+// FSLBM_PACKED=0 uses scalar pair arithmetic and FSLBM_TILE_Y=16|32 picks the column-pair kernel's tile height (for comparisons).
+static int configure_kernel(fslbm_solve* s) {
+  const char* ek = std::getenv("FSLBM_STEP_KERNEL");
+  const char* et = std::getenv("FSLBM_TILE_Y");
+  s->use2 = step2_supported(s->dtype, s->prm.d1) && !(ek && std::atoi(ek) == 1);
+  s->ty2 = (et && std::atoi(et) == 16) ? 16 : 32;
+  const char* ep = std::getenv("FSLBM_PACKED");
+  s->packed2 = (ep && std::atoi(ep) == 0) ? 0 : 1;
+  const std::vector<int2> tiles = fluid_tiles(s, s->use2 ? s->ty2 : kTY);
+  if (s->d_tiles) {
+    cudaFree(s->d_tiles);
+    s->bytes_device -= int64_t(s->ntiles) * sizeof(int2);
+    s->d_tiles = nullptr;
+  }
+  s->ntiles = int(tiles.size());
+  CUDA_TRY(cudaMalloc(&s->d_tiles, tiles.size() * sizeof(int2)));
+  s->bytes_device += int64_t(tiles.size() * sizeof(int2));
+  CUDA_TRY(cudaMemcpy(s->d_tiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  if (s->use2) {
+    CUDA_TRY(step2_prepare(s->prm.d1, s->ty2));
+    // tiles x streamwise chunks, at most one CTA per SM slot and chunks of at least 2R planes
+    const int slots = s->ctx->sm_count * step2_occupancy(s->prm.d1, s->ty2);
+    int nch = std::max(1, slots / s->ntiles);
+    nch = std::min(nch, std::max(1, s->L / (4 * s->prm.d1)));
+    s->grid2 = s->ntiles * nch;
+  } else {
+    CUDA_TRY(step_prepare(s->dtype, s->prm.d1));
+    choose_chunks(s);
+  }
+  return build_tensor_maps(s);
 }
 
 // Static wall sums per column (see step_kernel.cuh): sums of w(cx)w(cy) cx^a cy^b over the
@@ -326,17 +397,6 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
     if (s->sy >= s->ly) s->sy = s->ly - 1;
     s->sz = s->L / 2;
   }
-  // tiles that contain fluid
-  std::vector<int2> tiles;
-  for (int y0 = 0; y0 < s->ly; y0 += kTY)
-    for (int x0 = 0; x0 < s->lxp; x0 += kTX) {
-      bool any = false;
-      for (int y = y0; y < std::min(y0 + kTY, s->ly) && !any; ++y)
-        for (int x = x0; x < std::min(x0 + kTX, s->lxp); ++x)
-          if (s->mask[size_t(y) * s->lxp + x] == 0) { any = true; break; }
-      if (any) tiles.push_back(make_int2(x0, y0));
-    }
-  s->ntiles = int(tiles.size());
 
   const size_t fs = field_stride(s);
   cudaError_t e = cudaSuccess;
@@ -360,8 +420,6 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
     if ((e = dalloc(s, &s->d_colcoef, cc.size() * sizeof(cc[0])))) return fail("colcoef");
     cudaMemcpy(s->d_colcoef, cc.data(), cc.size() * sizeof(cc[0]), cudaMemcpyHostToDevice);
   }
-  if ((e = dalloc(s, &s->d_tiles, tiles.size() * sizeof(int2)))) return fail("tiles");
-  cudaMemcpy(s->d_tiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice);
   if ((e = dalloc(s, &s->d_counters, sizeof(DevCounters)))) return fail("counters");
   cudaMemset(s->d_counters, 0, sizeof(DevCounters));
   if ((e = dalloc(s, &s->d_log, sizeof(fslbm_monitor) * s->log_cap))) return fail("log");
@@ -371,9 +429,7 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
   cudaMemset(s->d_err, 0, sizeof(unsigned));
   if ((e = dalloc(s, &s->d_scratch, 8 * sizeof(double)))) return fail("scratch");
   if ((e = cudaEventCreate(&s->ev0)) || (e = cudaEventCreate(&s->ev1))) return fail("events");
-  if ((e = step_prepare(dtype, prm->d1))) return fail("step_prepare");
-  if (int r = build_tensor_maps(s)) { free_solve(s); return r; }
-  choose_chunks(s);
+  if (int r = configure_kernel(s)) { free_solve(s); return r; }
   if ((e = cudaDeviceSynchronize())) return fail("set-up");
   *out = s;
   return FSLBM_OK;
@@ -393,9 +449,7 @@ extern "C" int fslbm_solve_set_params(fslbm_solve* s, const fslbm_params* prm) {
   if (d1_changed) {
     CUDA_TRY(cudaSetDevice(s->ctx->device));
     CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
-    CUDA_TRY(step_prepare(s->dtype, prm->d1));
-    if (int r = build_tensor_maps(s)) return r;
-    choose_chunks(s);
+    if (int r = configure_kernel(s)) return r;
   }
   return FSLBM_OK;
 }
@@ -532,7 +586,12 @@ static int enqueue_steps(fslbm_solve* s, int64_t nsteps) {
       }
       CUDA_TRY(cudaEventRecord(s->tev[s->tev_used], st));
     }
-    CUDA_TRY(launch_step(a, st));
+    if (s->use2) {
+      Step2Launch b2{s->prm.d1, s->ty2, s->packed2, &s->maps2p[s->cur], &s->maps2u[s->cur], s->grid2};
+      CUDA_TRY(launch_step2(a, b2, st));
+    } else {
+      CUDA_TRY(launch_step(a, st));
+    }
     if (s->timing) {
       CUDA_TRY(cudaEventRecord(s->tev[s->tev_used + 1], st));
       s->tev_used += 2;

@@ -3,6 +3,7 @@
 #include <cstdio>
 #include "internal.h"
 #include "step_kernel.cuh"
+#include "step2_kernel.cuh"
 
 namespace fslbm {
 
@@ -77,6 +78,68 @@ cudaError_t launch_step(const StepLaunch& a, cudaStream_t st) {
     if (a.d1 == 2) return launch_step_t<double, 2>(a, st);
   }
   return cudaErrorInvalidValue;
+}
+
+// ------------------------------------------------------------------------------------------
+// FP32 column-pair kernel dispatch
+// ------------------------------------------------------------------------------------------
+bool step2_supported(int dtype, int d1) { return dtype == FSLBM_F32 && d1 == 2; }
+
+template <int TY> static void box2(int* sw, int* ph, int* uh, int* hx, int* hy) {
+  using Tl = Step2Tile<2, TY>;
+  *sw = Tl::SW; *ph = Tl::PH; *uh = Tl::UH; *hx = Tl::HX; *hy = Tl::HY;
+}
+
+bool step2_box(int d1, int ty, int* sw, int* ph, int* uh, int* hx, int* hy) {
+  if (d1 != 2) return false;
+  if (ty == 32) { box2<32>(sw, ph, uh, hx, hy); return true; }
+  if (ty == 16) { box2<16>(sw, ph, uh, hx, hy); return true; }
+  return false;
+}
+
+int step2_occupancy(int, int) { return 1; }
+
+template <int TY, bool PK> static cudaError_t prep2() {
+  return cudaFuncSetAttribute(fslbm_step2_kernel<2, TY, PK>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(Step2Tile<2, TY>::SMEM_BYTES));
+}
+
+cudaError_t step2_prepare(int d1, int ty) {
+  if (d1 != 2) return cudaErrorInvalidValue;
+  cudaError_t e;
+  if (ty == 32) {
+    if ((e = prep2<32, true>())) return e;
+    return prep2<32, false>();
+  }
+  if (ty == 16) {
+    if ((e = prep2<16, true>())) return e;
+    return prep2<16, false>();
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_step2(const StepLaunch& a, const Step2Launch& b, cudaStream_t st) {
+  Step2Geom g;
+  g.lxp = a.lxp; g.ly = a.ly; g.L = a.L; g.ntiles = a.ntiles; g.nchunks = b.grid / a.ntiles;
+  g.tiles = a.tiles; g.mask = a.mask; g.colcoef = a.colcoef; g.out = a.out;
+  g.gauge = a.gauge; g.err = a.err;
+  g.step_counter = a.counters ? &a.counters->steps : nullptr;
+  StepConst<float> k;
+  k.tb = float(a.tb); k.cc = float(a.cc); k.pin = float(a.pin); k.dtddy = float(a.dtddy);
+  k.m = float(a.m); k.c0 = float(a.c0); k.c1 = float(a.c1); k.c2 = float(a.c2);
+  k.fx = float(a.fx); k.fy = float(a.fy); k.fz = float(a.fz);
+#define FSLBM_L2(TY, PK)                                                                        \
+  fslbm_step2_kernel<2, TY, PK><<<b.grid, Step2Tile<2, TY>::THREADS, Step2Tile<2, TY>::SMEM_BYTES, \
+                                  st>>>(*b.map_p, *b.map_uvw, g, k)
+  if (b.d1 != 2) return cudaErrorInvalidValue;
+  if (b.ty == 32 && b.packed) FSLBM_L2(32, true);
+  else if (b.ty == 32) FSLBM_L2(32, false);
+  else if (b.ty == 16 && b.packed) FSLBM_L2(16, true);
+  else if (b.ty == 16) FSLBM_L2(16, false);
+  else return cudaErrorInvalidValue;
+#undef FSLBM_L2
+  return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------------------------------
