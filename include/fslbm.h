@@ -173,6 +173,30 @@ int fslbm_batch_destroy(fslbm_batch* b);
 int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int use_graph);
 int fslbm_batch_sync(fslbm_batch* b);
 
+/* ---- allocation-free step ---- */
+/* No counterpart in the reference. Advances a caller-owned FP32 state by one step (the same
+ * fused kernel as fslbm_solve_step, d1 = 2) without allocating device memory, for callers that
+ * cannot let a library call cudaMalloc: applications that give all device memory to their own
+ * pool, or that step inside a loop where an allocation (which may synchronise the device and
+ * fail under memory pressure) is not allowed.
+ *  - state_in, state_out: device arrays of 4 fields (p,u,v,w), each lz*ly*lx_pitch floats, x
+ *    fastest, field stride lz*ly*lx_pitch; 16-byte aligned; lx_pitch a multiple of 8, >= lx.
+ *    Wall cells and the padding columns x >= lx must hold zero in state_in; the step does not
+ *    write them in state_out, so keep them zero there too (for example by zeroing it once).
+ *  - mask: device array of ly*lx_pitch bytes, 0 fluid / 125 wall; padding columns are wall.
+ *  - gauge: p2 subtracted from p this step (0 outside the step after a monitor).
+ *  - stream: the caller's cudaStream_t (NULL for the default stream). The call returns after
+ *    the step has finished on that stream.
+ * Limit: lx_pitch*ly <= 65536 cells; larger cross-sections return FSLBM_ERR_ARG. The work
+ * tables live in a preallocated device array of about 1 MiB that every GPU loading the library
+ * holds until exit; every call reuses it and overwrites its contents, so calls that overlap on
+ * the GPU (on unordered streams) race. The first call on a device sets up that device (it looks
+ * up the array's address and the kernel's attributes); make that first call before any stream
+ * capture on the device. */
+int fslbm_step_f32_noalloc(const float* state_in, float* state_out, const uint8_t* mask, int lx,
+                           int ly, int lz, int lx_pitch, const fslbm_params* prm, double gauge,
+                           void* stream);
+
 /* ---- host-side formats and generators ---- */
 /* pipe.txt: one integer per line, x fastest (pipe.m:62). Reads exactly lx*ly*lz values; extra
  * or missing values are an FSLBM_ERR_IO (the reference's feof loop writes one byte past its
