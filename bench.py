@@ -138,7 +138,7 @@ class ClockSampler:
 
 def read_traffic():
     """DRAM bytes per step-kernel launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "fslbm_step_f32_512x128x128.md")
+    path = os.path.join(ROOT, "profiles", "fslbm_step2_f32_512x128x128.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -327,7 +327,7 @@ def run_ours(args, rank, world, local):
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic,
                              "peak_source": f"{peak_kind} hbm_gbs",
-                             "kernel": "fslbm_step_kernel<float,2>",
+                             "kernel": "fslbm_step2_kernel<2,32,packed>",
                              "kernel_ms_avg": kern_avg_ms, "algorithmic_bytes": alg_bytes},
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "max_abs_u": umax_now}
