@@ -19,6 +19,7 @@
 //  - warps whose columns are all wall keep the pipeline protocol but skip the arithmetic.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include "common.h"
@@ -123,6 +124,7 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY>::THREADS, 1)
                        const StepConst<float> k) {
   using Tl = Step2Tile<D1, TY>;
   using F = Pair<PK>;
+  static_assert(D1 == 2, "the march prologue below is written for d1 = 2 (R = 4)");
   constexpr int R = Tl::R, HX = Tl::HX, HY = Tl::HY, SW = Tl::SW, S = Tl::S, AH = Tl::AHEAD;
   constexpr int PPL = Tl::PPLANE, UPL = Tl::UPLANE, SLOT = Tl::SLOT;
 
@@ -143,27 +145,16 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY>::THREADS, 1)
   const int start = dir > 0 ? zb - R : ze - 1 + R;      // real plane of march index 0
   const int2 org = g.tiles[tile];
   const int xa = org.x + 2 * tp, y = org.y + ty;
+  const bool inside = xa < g.lxp && y < g.ly;
 
   float2 ws0 = f2(0.f), wsx = f2(0.f), wsy = f2(0.f), fl = f2(0.f);
-  if (xa < g.lxp && y < g.ly) {
+  if (inside) {
     const ColCoef<float>* cp = reinterpret_cast<const ColCoef<float>*>(g.colcoef) + size_t(y) * g.lxp + xa;
     const ColCoef<float> ca = cp[0], cb = cp[1];
     ws0 = make_float2(ca.ws0, cb.ws0); wsx = make_float2(ca.wsx, cb.wsx);
     wsy = make_float2(ca.wsy, cb.wsy); fl = make_float2(ca.fluid, cb.fluid);
   }
-  const bool fluid_any = fl.x != 0.f || fl.y != 0.f;
-  const bool warp_on = __any_sync(0xffffffffu, fluid_any);
-  // non-wall flags of the 4 x 3 neighbourhood (columns xa-1..xa+2), for the seam jump
-  unsigned nwbits = 0;
-  if (warp_on) {
-    for (int cy = -1; cy <= 1; ++cy)
-      for (int j = 0; j < 4; ++j) {
-        const int gx = xa - 1 + j, gy = y + cy;
-        const bool nwall = gx >= 0 && gy >= 0 && gx < g.lxp && gy < g.ly &&
-                           g.mask[size_t(gy) * g.lxp + gx] != kWall;
-        nwbits |= unsigned(nwall) << ((cy + 1) * 4 + j);
-      }
-  }
+  const bool warp_on = __any_sync(0xffffffffu, fl.x != 0.f || fl.y != 0.f);
 
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
@@ -194,165 +185,247 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY>::THREADS, 1)
       for (int q = from; q <= issued; ++q)
         mbar_wait_bounded(&full[q & (S - 1)], uint32_t((q / S) & 1), kWaitLimitNs / 8);
   };
-
-  const float gauge = g.gauge ? float(*g.gauge) : 0.0f;
-  const size_t FS = size_t(g.lxp) * g.ly * g.L;
-  float* out = reinterpret_cast<float*>(g.out);
-  // true predictor sums from the row-factored ones: A0/36, dir*A1'/12, A2'/8
-  const float2 s0 = f2(1.0f / 36.0f), s1 = f2(float(dir) / 12.0f), s2 = f2(1.0f / 8.0f);
-  const int po = (ty + 1) * SW + HX + 2 * tp;                 // p box
-  const int uo = PPL + (ty + HY) * SW + HX + 2 * tp;          // u box (v, w at +UPL, +2 UPL)
-
-  float2 hu[R], hv[R], hw[R];                                 // own columns, march planes j-R..j-1
-#pragma unroll
-  for (int j = 0; j < R; ++j) { hu[j] = f2(0.f); hv[j] = f2(0.f); hw[j] = f2(0.f); }
-  float2 aA[4], aB[4];
-#pragma unroll
-  for (int j = 0; j < 4; ++j) { aA[j] = f2(0.f); aB[j] = f2(0.f); }
-
-  for (int m = 0; m < niter; ++m) {
-    if (!mbar_wait_bounded(&full[m & (S - 1)], uint32_t((m / S) & 1), kWaitLimitNs)) {
-      if (lane == 0) atomicOr(g.err, 1u);
-      drain(m + 1);
-      return;
-    }
-    const int ma = m - R + 1;                                 // predictor plane (march index)
-    const int jo = m - R;                                     // output plane (march index)
-    if (warp_on) {
-      float2 comp0 = f2(0.f), comp1 = f2(0.f), comp2 = f2(0.f), comp3 = f2(0.f);
-      if (ma >= R - 1) {
-        const float* ss = ring + (ma & (S - 1)) * SLOT;
-        const int sp = start + dir * ma;                      // real plane
-        const float off = sp < 0 ? k.pin : (sp >= g.L ? -k.pin : 0.0f);
-        // row-factored weights w(cx)w(cy) = {4,1,1}x{4,1,1}/36: per row R = P(-1)+P(+1)+4P(0),
-        // D = P(+1)-P(-1); across rows A = R(-1)+R(+1)+4R(0), X likewise on D, Y = R(+1)-R(-1)
-        float2 A[3], X[3], Y[3];
-#pragma unroll
-        for (int cy = -1; cy <= 1; ++cy) {
-          const float* rp = ss + po + cy * SW;
-          const float* rq = ss + uo + cy * SW;
-          const float2 pL = lds2(rp - 2), pC = lds2(rp), pR = lds2(rp + 2);
-          const float2 uL = lds2(rq - 2), uC = lds2(rq), uR = lds2(rq + 2);
-          const float2 vL = lds2(rq + UPL - 2), vC = lds2(rq + UPL), vR = lds2(rq + UPL + 2);
-          const float2 wL = lds2(rq + 2 * UPL - 2), wC = lds2(rq + 2 * UPL), wR = lds2(rq + 2 * UPL + 2);
-          float2 pm = make_float2(pL.y, pC.x), p0 = pC, pp = make_float2(pC.y, pR.x);
-          if (off != 0.0f) {
-            const unsigned bb = nwbits >> ((cy + 1) * 4);
-            pm.x += (bb & 1u) ? off : 0.f; pm.y += (bb & 2u) ? off : 0.f;
-            p0.x += (bb & 2u) ? off : 0.f; p0.y += (bb & 4u) ? off : 0.f;
-            pp.x += (bb & 4u) ? off : 0.f; pp.y += (bb & 8u) ? off : 0.f;
-          }
-          const float2 um = make_float2(uL.y, uC.x), up = make_float2(uC.y, uR.x);
-          const float2 vm = make_float2(vL.y, vC.x), vp = make_float2(vC.y, vR.x);
-          const float2 wm = make_float2(wL.y, wC.x), wp = make_float2(wC.y, wR.x);
-          float2 Pm[3], P0[3], Pp[3];
-          if (cy == -1) {
-            brackets<PK, -1, -1>(qof<PK>(pm, um, vm, wm), um, vm, wm, Pm[0], Pm[1], Pm[2]);
-            brackets<PK, 0, -1>(qof<PK>(p0, uC, vC, wC), uC, vC, wC, P0[0], P0[1], P0[2]);
-            brackets<PK, 1, -1>(qof<PK>(pp, up, vp, wp), up, vp, wp, Pp[0], Pp[1], Pp[2]);
-          } else if (cy == 0) {
-            brackets<PK, -1, 0>(qof<PK>(pm, um, vm, wm), um, vm, wm, Pm[0], Pm[1], Pm[2]);
-            brackets<PK, 0, 0>(qof<PK>(p0, uC, vC, wC), uC, vC, wC, P0[0], P0[1], P0[2]);
-            brackets<PK, 1, 0>(qof<PK>(pp, up, vp, wp), up, vp, wp, Pp[0], Pp[1], Pp[2]);
-          } else {
-            brackets<PK, -1, 1>(qof<PK>(pm, um, vm, wm), um, vm, wm, Pm[0], Pm[1], Pm[2]);
-            brackets<PK, 0, 1>(qof<PK>(p0, uC, vC, wC), uC, vC, wC, P0[0], P0[1], P0[2]);
-            brackets<PK, 1, 1>(qof<PK>(pp, up, vp, wp), up, vp, wp, Pp[0], Pp[1], Pp[2]);
-          }
-#pragma unroll
-          for (int q = 0; q < 3; ++q) {
-            const float2 Rq = F::fma(f2(4.0f), P0[q], F::add(Pm[q], Pp[q]));
-            const float2 Dq = F::fma(f2(-1.0f), Pm[q], Pp[q]);
-            if (cy == -1) { A[q] = Rq; X[q] = Dq; Y[q] = Rq; }
-            else if (cy == 0) { A[q] = F::fma(f2(4.0f), Rq, A[q]); X[q] = F::fma(f2(4.0f), Dq, X[q]); }
-            else { A[q] = F::add(A[q], Rq); X[q] = F::add(X[q], Dq); Y[q] = F::fma(f2(-1.0f), Y[q], Rq); }
-          }
-        }
-        const float2 tA0 = F::mul(A[0], s0), tA1 = F::mul(A[1], s1), tA2 = F::mul(A[2], s2);
-        const float2 tX0 = F::mul(X[0], s0), tX1 = F::mul(X[1], s1), tX2 = F::mul(X[2], s2);
-        const float2 tY0 = F::mul(Y[0], s0), tY1 = F::mul(Y[1], s1), tY2 = F::mul(Y[2], s2);
-        // plane ma is the march-next neighbour of output ma-1 (completed here), itself, and
-        // the march-previous neighbour of ma+1
-        const float2 A02 = F::add(tA0, tA2), X02 = F::add(tX0, tX2), Y02 = F::add(tY0, tY2);
-        const float2 sP = F::add(A02, tA1), sM = F::fma(tA1, f2(-1.f), A02);
-        const float2 xP = F::add(X02, tX1), xM = F::fma(tX1, f2(-1.f), X02);
-        const float2 yP = F::add(Y02, tY1), yM = F::fma(tY1, f2(-1.f), Y02);
-        const float2 cw0 = f2(2.0f / 3.0f), cw1 = f2(1.0f / 6.0f);
-        comp0 = F::fma(cw1, sP, aA[0]);
-        comp1 = F::fma(cw1, xP, aA[1]);
-        comp2 = F::fma(cw1, yP, aA[2]);
-        comp3 = F::fma(cw1, sP, aA[3]);
-        aA[0] = F::fma(cw0, tA0, aB[0]);
-        aA[1] = F::fma(cw0, tX0, aB[1]);
-        aA[2] = F::fma(cw0, tY0, aB[2]);
-        aA[3] = aB[3];
-        aB[0] = F::mul(cw1, sM);
-        aB[1] = F::mul(cw1, xM);
-        aB[2] = F::mul(cw1, yM);
-        aB[3] = F::mul(f2(-1.0f / 6.0f), sM);
-      }
-      if (jo >= 0) {
-        const float* so = ring + (jo & (S - 1)) * SLOT;
-        const float2 uc = lds2(so + uo), vc = lds2(so + uo + UPL), wc = lds2(so + uo + 2 * UPL);
-        if (jo >= R && fluid_any) {
-          // ---- output plane: corrector and update
-          const float* sa1 = ring + ((jo + D1) & (S - 1)) * SLOT;   // march planes ahead
-          const float* sa2 = ring + ((jo + 2 * D1) & (S - 1)) * SLOT;
-          const float2 pc = lds2(so + po);
-          auto lap = [&](int f, float2 c, float2 zb1, float2 zb2) {
-            const float* q = so + uo + f * UPL;
-            const float2 za1 = lds2(sa1 + uo + f * UPL), za2 = lds2(sa2 + uo + f * UPL);
-            const float2 t1 = F::add(F::add(F::add(lds2(q - D1), lds2(q + D1)),
-                                            F::add(lds2(q - D1 * SW), lds2(q + D1 * SW))),
-                                     F::add(zb1, za1));
-            const float2 t2 = F::add(F::add(F::add(lds2(q - 2 * D1), lds2(q + 2 * D1)),
-                                            F::add(lds2(q - 2 * D1 * SW), lds2(q + 2 * D1 * SW))),
-                                     F::add(zb2, za2));
-            return F::fma(f2(k.c2), t2, F::fma(f2(k.c1), t1, F::mul(f2(k.c0), c)));
-          };
-          const float2 Lu = lap(0, uc, hu[R - D1], hu[0]);
-          const float2 Lv = lap(1, vc, hv[R - D1], hv[0]);
-          const float2 Lw = lap(2, wc, hw[R - D1], hw[0]);
-          const float2 rho = F::add(F::fma(pc, ws0, comp0), f2(-gauge));
-          const float2 us = F::fma(pc, wsx, comp1), vs = F::fma(pc, wsy, comp2);
-          const float2 wsz = F::mul(comp3, f2(float(dir)));
-          const float2 dt = f2(k.dtddy), mm = f2(k.m), tb = f2(k.tb), cc = f2(k.cc);
-          const float2 un = F::fma(F::add(F::fma(F::mul(dt, Lu), mm, us), f2(k.fx)), tb, F::mul(uc, cc));
-          const float2 vn = F::fma(F::add(F::fma(F::mul(dt, Lv), mm, vs), f2(k.fy)), tb, F::mul(vc, cc));
-          const float2 wn = F::fma(F::add(F::fma(F::mul(dt, Lw), mm, wsz), f2(k.fz)), tb, F::mul(wc, cc));
-          const int zo = start + dir * jo;
-          const size_t o = (size_t(zo) * g.ly + y) * g.lxp + xa;
-          auto put = [&](float* dst, float2 v) {
-            v.x = fl.x != 0.f ? v.x : 0.f;
-            v.y = fl.y != 0.f ? v.y : 0.f;
-            *reinterpret_cast<float2*>(dst) = v;
-          };
-          put(out + o, rho);
-          put(out + FS + o, un);
-          put(out + 2 * FS + o, vn);
-          put(out + 3 * FS + o, wn);
-        }
-        // own columns of plane jo join the history of streamwise taps
-#pragma unroll
-        for (int j = 0; j < R - 1; ++j) { hu[j] = hu[j + 1]; hv[j] = hv[j + 1]; hw[j] = hw[j + 1]; }
-        hu[R - 1] = uc; hv[R - 1] = vc; hw[R - 1] = wc;
-      }
-    }
-    // plane jo leaves the window: release its slot, then refill it with march plane m + AH + 1
+  // wait for march plane m; false after flagging a failure (the caller returns)
+  auto arrive_wait = [&](int m) -> bool {
+    if (mbar_wait_bounded(&full[m & (S - 1)], uint32_t((m / S) & 1), kWaitLimitNs)) return true;
+    if (lane == 0) atomicOr(g.err, 1u);
+    drain(m + 1);
+    return false;
+  };
+  // plane m - R leaves the window: release its slot; thread 0 refills it with plane m + AH + 1
+  auto release_produce = [&](int m) -> bool {
     __syncwarp();
-    if (jo >= 0 && lane == 0) mbar_arrive(&empty[jo & (S - 1)]);
+    if (m >= R && lane == 0) mbar_arrive(&empty[(m - R) & (S - 1)]);
     if (tid == 0 && m + AH + 1 < niter) {
       const int mn = m + AH + 1;
       if (mn >= S &&
           !mbar_wait_bounded(&empty[mn & (S - 1)], uint32_t(((mn - S) / S) & 1), kWaitLimitNs)) {
         atomicOr(g.err, 1u);
         drain(m + 1);
-        return;
+        return false;
       }
       fence_proxy_async_smem();
       issue(mn);
       issued = mn;
     }
+    return true;
+  };
+
+  if (!warp_on) {   // all-wall warps keep the pipeline protocol only
+    for (int m = 0; m < niter; ++m)
+      if (!arrive_wait(m) || !release_produce(m)) return;
+    return;
+  }
+
+  const float gauge = g.gauge ? float(*g.gauge) : 0.0f;
+  const size_t FS = size_t(g.lxp) * g.ly * g.L;
+  float* outp = reinterpret_cast<float*>(g.out) + (size_t(start + dir * R) * g.ly + y) * g.lxp + xa;
+  const long long ostep = (long long)dir * g.ly * g.lxp;     // output pointer step per plane
+  const int po = (ty + 1) * SW + HX + 2 * tp;                 // p box
+  const int uo = PPL + (ty + HY) * SW + HX + 2 * tp;          // u box (v, w at +UPL, +2 UPL)
+  // seam pressure jump: a wrapped plane adds off to p on its non-wall cells, i.e. off times the
+  // non-wall weight sums (raw units, x36) to the row-factored A0, X0, Y0
+  const float n0[2] = {36.f - 36.f * ws0.x, 36.f - 36.f * ws0.y};
+  const float nx[2] = {-36.f * wsx.x, -36.f * wsx.y};
+  const float ny[2] = {-36.f * wsy.x, -36.f * wsy.y};
+  const float h6 = float(dir) / 72.0f;
+
+  float2 hu[4], hv[4], hw[4];                                 // own columns of planes jo-4..jo-1
+  float aA[4][2], aB[4][2];                                   // predictor sums of the next outputs
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    hu[j] = hv[j] = hw[j] = f2(0.f);
+    aA[j][0] = aA[j][1] = aB[j][0] = aB[j][1] = 0.f;
+  }
+  float2 comp0, comp1, comp2, comp3;
+
+  // predictor contribution of march plane ma (see step_kernel.cuh for the factorisation)
+  auto predictor = [&](int ma) {
+    const float* ss = ring + (ma & (S - 1)) * SLOT;
+    const int sp = start + dir * ma;                          // real plane
+    const float off = sp < 0 ? k.pin : (sp >= g.L ? -k.pin : 0.0f);
+    // Row-factored weights w(cx)w(cy) = {4,1,1}x{4,1,1}/36, per column of the pair: per row
+    // R = P(-1)+P(+1)+4P(0), D = P(+1)-P(-1); across rows A = R(-1)+R(+1)+4R(0), X likewise on
+    // D, Y = R(+1)-R(-1). The four cells x-1..x+2 of a row are shared by the two columns, so q
+    // and w^2 are formed once per cell.
+    float A[2][3], X[2][3], Y[2][3];
+#pragma unroll
+    for (int cy = -1; cy <= 1; ++cy) {
+      const float* rp = ss + po + cy * SW;
+      const float* rq = ss + uo + cy * SW;
+      const float2 pL = lds2(rp - 2), pC = lds2(rp), pR = lds2(rp + 2);
+      const float2 uL = lds2(rq - 2), uC = lds2(rq), uR = lds2(rq + 2);
+      const float2 vL = lds2(rq + UPL - 2), vC = lds2(rq + UPL), vR = lds2(rq + UPL + 2);
+      const float2 wL = lds2(rq + 2 * UPL - 2), wC = lds2(rq + 2 * UPL), wR = lds2(rq + 2 * UPL + 2);
+      const float pc4[4] = {pL.y, pC.x, pC.y, pR.x};
+      const float uc4[4] = {uL.y, uC.x, uC.y, uR.x};
+      const float vc4[4] = {vL.y, vC.x, vC.y, vR.x};
+      const float wc4[4] = {wL.y, wC.x, wC.y, wR.x};
+      float q4[4], w24[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        w24[j] = wc4[j] * wc4[j];
+        q4[j] = __fmaf_rn(-1.5f, __fmaf_rn(uc4[j], uc4[j], __fmaf_rn(vc4[j], vc4[j], w24[j])), pc4[j]);
+      }
+#pragma unroll
+      for (int col = 0; col < 2; ++col) {
+        float P[3][3];   // [cx+1][k]
+#pragma unroll
+        for (int cx = -1; cx <= 1; ++cx) {
+          const int j = col + 1 + cx;
+          const float u = uc4[j], v = vc4[j], w = wc4[j];
+          float P0, P1;
+          if (cx == 0 && cy == 0) {
+            P0 = q4[j];
+            P1 = w;
+          } else if (cx == 0 || cy == 0) {
+            const float Bv = cy == 0 ? u : v;
+            const float s3 = 3.0f * float(cx + cy);
+            P0 = __fmaf_rn(Bv, __fmaf_rn(Bv, 4.5f, s3), q4[j]);
+            P1 = w * __fmaf_rn(Bv, s3, 1.0f);
+          } else {
+            const float a1 = __fmaf_rn(v, float(cx * cy), u);
+            const float s3 = 3.0f * float(cx);
+            P0 = __fmaf_rn(a1, __fmaf_rn(a1, 4.5f, s3), q4[j]);
+            P1 = w * __fmaf_rn(a1, s3, 1.0f);
+          }
+          P[cx + 1][0] = P0; P[cx + 1][1] = P1; P[cx + 1][2] = w24[j];
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const float Rq = __fmaf_rn(4.0f, P[1][q], P[0][q] + P[2][q]);
+          const float Dq = P[2][q] - P[0][q];
+          if (cy == -1) { A[col][q] = Rq; X[col][q] = Dq; Y[col][q] = Rq; }
+          else if (cy == 0) { A[col][q] = __fmaf_rn(4.0f, Rq, A[col][q]); X[col][q] = __fmaf_rn(4.0f, Dq, X[col][q]); }
+          else { A[col][q] += Rq; X[col][q] += Dq; Y[col][q] = Rq - Y[col][q]; }
+        }
+      }
+    }
+    // True sums are A0'/36, dir A1'/12, A2'/8 (P1 and P2 were formed as P1/3 and P2/4.5).
+    // Plane ma is the march-next neighbour of output ma-1 (completed here), itself, and the
+    // march-previous neighbour of ma+1: with e = (A0 + A2)/6 and h = A1/6,
+    // comp += e + h, aA = aB + (2/3) A0, aB = e - h (z-moment: comp += e + h, aB = h - e).
+    float cmp[4][2];
+#pragma unroll
+    for (int col = 0; col < 2; ++col) {
+      const float A0 = __fmaf_rn(off, n0[col], A[col][0]);
+      const float X0 = __fmaf_rn(off, nx[col], X[col][0]);
+      const float Y0 = __fmaf_rn(off, ny[col], Y[col][0]);
+      const float eA = __fmaf_rn(A[col][2], 1.0f / 48.0f, A0 * (1.0f / 216.0f));
+      const float hA = A[col][1] * h6;
+      const float eX = __fmaf_rn(X[col][2], 1.0f / 48.0f, X0 * (1.0f / 216.0f));
+      const float hX = X[col][1] * h6;
+      const float eY = __fmaf_rn(Y[col][2], 1.0f / 48.0f, Y0 * (1.0f / 216.0f));
+      const float hY = Y[col][1] * h6;
+      const float sA = eA + hA;
+      cmp[0][col] = aA[0][col] + sA;
+      cmp[1][col] = aA[1][col] + (eX + hX);
+      cmp[2][col] = aA[2][col] + (eY + hY);
+      cmp[3][col] = aA[3][col] + sA;
+      aA[0][col] = __fmaf_rn(A0, 1.0f / 54.0f, aB[0][col]);
+      aA[1][col] = __fmaf_rn(X0, 1.0f / 54.0f, aB[1][col]);
+      aA[2][col] = __fmaf_rn(Y0, 1.0f / 54.0f, aB[2][col]);
+      aA[3][col] = aB[3][col];
+      aB[0][col] = eA - hA;
+      aB[1][col] = eX - hX;
+      aB[2][col] = eY - hY;
+      aB[3][col] = hA - eA;
+    }
+    comp0 = make_float2(cmp[0][0], cmp[0][1]);
+    comp1 = make_float2(cmp[1][0], cmp[1][1]);
+    comp2 = make_float2(cmp[2][0], cmp[2][1]);
+    comp3 = make_float2(cmp[3][0], cmp[3][1]);
+  };
+
+  // own columns of march plane jo (for the history)
+  auto own = [&](int jo, float2& uc, float2& vc, float2& wc) {
+    const float* so = ring + (jo & (S - 1)) * SLOT;
+    uc = lds2(so + uo); vc = lds2(so + uo + UPL); wc = lds2(so + uo + 2 * UPL);
+  };
+
+  // corrector and update of output march plane jo; hist slot ROT holds plane jo-4 and is then
+  // overwritten with plane jo
+  auto output = [&](int jo, auto rot_c) {
+    constexpr int ROT = decltype(rot_c)::value;
+    const float* so = ring + (jo & (S - 1)) * SLOT;
+    const float* sa1 = ring + ((jo + D1) & (S - 1)) * SLOT;   // march planes ahead
+    const float* sa2 = ring + ((jo + 2 * D1) & (S - 1)) * SLOT;
+    const float2 pc = lds2(so + po);
+    const float2 uc = lds2(so + uo), vc = lds2(so + uo + UPL), wc = lds2(so + uo + 2 * UPL);
+    auto lap = [&](int f, float2 c, float2 zb1, float2 zb2) {
+      const float* q = so + uo + f * UPL;
+      const float2 za1 = lds2(sa1 + uo + f * UPL), za2 = lds2(sa2 + uo + f * UPL);
+      const float2 t1 = F::add(F::add(F::add(lds2(q - D1), lds2(q + D1)),
+                                      F::add(lds2(q - D1 * SW), lds2(q + D1 * SW))),
+                               F::add(zb1, za1));
+      const float2 t2 = F::add(F::add(F::add(lds2(q - 2 * D1), lds2(q + 2 * D1)),
+                                      F::add(lds2(q - 2 * D1 * SW), lds2(q + 2 * D1 * SW))),
+                               F::add(zb2, za2));
+      return F::fma(f2(k.c2), t2, F::fma(f2(k.c1), t1, F::mul(f2(k.c0), c)));
+    };
+    constexpr int H2 = (ROT + 2) & 3;                         // plane jo-2
+    const float2 Lu = lap(0, uc, hu[H2], hu[ROT]);
+    const float2 Lv = lap(1, vc, hv[H2], hv[ROT]);
+    const float2 Lw = lap(2, wc, hw[H2], hw[ROT]);
+    hu[ROT] = uc; hv[ROT] = vc; hw[ROT] = wc;
+    const float2 rho = F::add(F::fma(pc, ws0, comp0), f2(-gauge));
+    const float2 us = F::fma(pc, wsx, comp1), vs = F::fma(pc, wsy, comp2);
+    const float2 wsz = F::mul(comp3, f2(float(dir)));
+    const float2 dt = f2(k.dtddy), mm = f2(k.m), tb = f2(k.tb), cc = f2(k.cc);
+    const float2 un = F::fma(F::add(F::fma(F::mul(dt, Lu), mm, us), f2(k.fx)), tb, F::mul(uc, cc));
+    const float2 vn = F::fma(F::add(F::fma(F::mul(dt, Lv), mm, vs), f2(k.fy)), tb, F::mul(vc, cc));
+    const float2 wn = F::fma(F::add(F::fma(F::mul(dt, Lw), mm, wsz), f2(k.fz)), tb, F::mul(wc, cc));
+    if (inside) {   // wall columns get zero (fl = 0)
+      *reinterpret_cast<float2*>(outp) = F::mul(rho, fl);
+      *reinterpret_cast<float2*>(outp + FS) = F::mul(un, fl);
+      *reinterpret_cast<float2*>(outp + 2 * FS) = F::mul(vn, fl);
+      *reinterpret_cast<float2*>(outp + 3 * FS) = F::mul(wn, fl);
+    }
+    outp += ostep;
+  };
+
+  using I0 = std::integral_constant<int, 0>;
+  using I1 = std::integral_constant<int, 1>;
+  using I2 = std::integral_constant<int, 2>;
+  using I3 = std::integral_constant<int, 3>;
+  // ---- prologue (R = 4): planes 0..3 arrive; 4..5 enter the history; 6..7 also start the
+  // predictor sums of the first output
+#pragma unroll
+  for (int m = 0; m < 2 * R; ++m) {
+    if (!arrive_wait(m)) return;
+    if (m >= 2 * R - 2) predictor(m - R + 1);
+    if (m >= R) {
+      float2 uc, vc, wc;
+      own(m - R, uc, vc, wc);
+      const int h = (m - R) & 3;
+      if (h == 0) { hu[0] = uc; hv[0] = vc; hw[0] = wc; }
+      else if (h == 1) { hu[1] = uc; hv[1] = vc; hw[1] = wc; }
+      else if (h == 2) { hu[2] = uc; hv[2] = vc; hw[2] = wc; }
+      else { hu[3] = uc; hv[3] = vc; hw[3] = wc; }
+    }
+    if (!release_produce(m)) return;
+  }
+  // ---- steady state, four planes per pass (the history period)
+  for (int m = 2 * R; m < niter; m += 4) {
+    if (!arrive_wait(m)) return;
+    predictor(m - R + 1);
+    output(m - R, I0{});
+    if (!release_produce(m)) return;
+    if (m + 1 >= niter) break;
+    if (!arrive_wait(m + 1)) return;
+    predictor(m - R + 2);
+    output(m - R + 1, I1{});
+    if (!release_produce(m + 1)) return;
+    if (m + 2 >= niter) break;
+    if (!arrive_wait(m + 2)) return;
+    predictor(m - R + 3);
+    output(m - R + 2, I2{});
+    if (!release_produce(m + 2)) return;
+    if (m + 3 >= niter) break;
+    if (!arrive_wait(m + 3)) return;
+    predictor(m - R + 4);
+    output(m - R + 3, I3{});
+    if (!release_produce(m + 3)) return;
   }
 }
 
