@@ -119,6 +119,7 @@ def lib():
             "fslbm_batch_destroy": ([_vp], _i),
             "fslbm_batch_step": ([_vp, ctypes.c_int64, _i], _i),
             "fslbm_batch_sync": ([_vp], _i),
+            "fslbm_batch_elapsed": ([_vp, ctypes.POINTER(ctypes.c_double)], _i),
             "fslbm_read_pipe_txt": ([ctypes.c_char_p, _i, _i, _i, _vp], _i),
             "fslbm_write_pipe_txt": ([ctypes.c_char_p, _i, _i, _i, _vp], _i),
             "fslbm_read_param_txt": ([ctypes.c_char_p, ctypes.POINTER(Params)], _i),
@@ -387,6 +388,11 @@ class Batch:
 
     def sync(self):
         _check(lib().fslbm_batch_sync(self.handle))
+
+    def elapsed_ms(self):
+        ms = ctypes.c_double()
+        _check(lib().fslbm_batch_elapsed(self.handle, ctypes.byref(ms)))
+        return ms.value
 
     def close(self):
         if self.handle:

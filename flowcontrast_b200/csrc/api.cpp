@@ -163,6 +163,15 @@ struct fslbm_solve {
 
 static size_t field_stride(const fslbm_solve* s) { return size_t(s->lxp) * s->ly * s->L; }
 
+// Milliseconds between two events, if both were recorded. A failed query (events never
+// recorded) is cleared from the runtime's last-error slot, where a later launch check would
+// otherwise report it.
+static void elapsed_if_recorded(cudaEvent_t a, cudaEvent_t b, double* out) {
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, a, b) == cudaSuccess) *out = ms;
+  else (void)cudaGetLastError();
+}
+
 static int validate_params(const fslbm_params* p, int dtype) {
   if (!p) return fslbm_set_error(FSLBM_ERR_ARG, "params: null");
   if (!step_supported(dtype, p->d1))
@@ -623,8 +632,7 @@ extern "C" int fslbm_solve_sync(fslbm_solve* s) {
   if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "sync: null solve");
   CUDA_TRY(cudaSetDevice(s->ctx->device));
   CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
-  float ms = 0;
-  if (cudaEventElapsedTime(&ms, s->ev0, s->ev1) == cudaSuccess) s->last_ms = ms;
+  elapsed_if_recorded(s->ev0, s->ev1, &s->last_ms);
   unsigned err = 0;
   CUDA_TRY(cudaMemcpy(&err, s->d_err, sizeof err, cudaMemcpyDeviceToHost));
   if (err) {
@@ -910,42 +918,180 @@ extern "C" int fslbm_profile_reset(fslbm_solve* s) {
 }
 
 // ------------------------------------------------------------------------------------------
-// batched ensemble (first form: the members' steps enqueued back to back on one stream)
+// batched ensemble: all members' steps of one time step in one persistent launch (FP32,
+// d1 = 2), followed by one bookkeeping launch (step counters, monitors, gauges); two steps are
+// captured once as a CUDA graph and replayed. Members of other kinds step one after another.
 // ------------------------------------------------------------------------------------------
 struct fslbm_batch {
-  fslbm_ctx* ctx;
+  fslbm_ctx* ctx = nullptr;
   std::vector<fslbm_solve*> members;
+  bool fast = false;
+  void* d_members = nullptr;
+  BatchMon* d_mons = nullptr;
+  std::vector<unsigned char> h_members;
+  std::vector<BatchMon> h_mons;
+  int nitems = 0, grid = 0, packed = 1, chunk = 64;
+  cudaGraphExec_t exec2 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0;
 };
+
+static void free_batch(fslbm_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->ctx->device);
+  if (b->exec2) cudaGraphExecDestroy(b->exec2);
+  if (b->d_members) cudaFree(b->d_members);
+  if (b->d_mons) cudaFree(b->d_mons);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  delete b;
+}
+
+// Member descriptors for the members' current buffers and step counts.
+static int batch_upload(fslbm_batch* b) {
+  const size_t mbytes = batch_member_bytes();
+  const int n = int(b->members.size());
+  b->h_members.assign(mbytes * n, 0);
+  b->h_mons.resize(n);
+  int item = 0;
+  for (int i = 0; i < n; ++i) {
+    fslbm_solve* s = b->members[i];
+    StepLaunch a{};
+    a.dtype = s->dtype; a.d1 = s->prm.d1;
+    a.lxp = s->lxp; a.ly = s->ly; a.L = s->L; a.ntiles = s->ntiles;
+    a.tiles = s->d_tiles; a.mask = s->d_mask; a.colcoef = s->d_colcoef; a.err = s->d_err;
+    fill_constants(s, a);
+    int nch = (s->L + b->chunk - 1) / b->chunk;
+    nch = std::max(1, std::min(nch, std::max(1, s->L / (4 * s->prm.d1))));
+    CUDA_TRY(fill_batch_member(b->h_members.data() + mbytes * i, s->maps2p, s->maps2u, a,
+                               s->state[0], s->state[1], s->d_gauge, &s->d_counters->steps,
+                               s->prm.monitor_every, s->cur, nch, item));
+    item += s->ntiles * nch;
+    BatchMon& m = b->h_mons[i];
+    std::memset(&m, 0, sizeof m);
+    m.mon.dtype = s->dtype; m.mon.mask = s->d_mask;
+    m.mon.lxp = s->lxp; m.mon.lx = s->lx; m.mon.ly = s->ly; m.mon.L = s->L;
+    m.mon.pin = double(float(s->prm.pin)); m.mon.nu = s->prm.nu; m.mon.radius = s->radius;
+    m.mon.l1 = double(s->fluid2d); m.mon.sx = s->sx; m.mon.sy = s->sy; m.mon.sz = s->sz;
+    m.mon.log = s->d_log; m.mon.log_cap = s->log_cap; m.mon.gauge_out = s->d_gauge;
+    m.mon.counters = s->d_counters;
+    m.state[0] = s->state[0]; m.state[1] = s->state[1];
+    m.monitor_every = s->prm.monitor_every; m.cur0 = s->cur;
+  }
+  b->nitems = item;
+  b->grid = std::max(1, std::min(item, b->ctx->sm_count));
+  cudaStream_t st = b->ctx->stream;
+  CUDA_TRY(cudaMemcpyAsync(b->d_members, b->h_members.data(), b->h_members.size(),
+                           cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(b->d_mons, b->h_mons.data(), sizeof(BatchMon) * n,
+                           cudaMemcpyHostToDevice, st));
+  return FSLBM_OK;
+}
+
+static cudaError_t batch_enqueue_one(fslbm_batch* b, int parity, cudaStream_t st) {
+  cudaError_t e = launch_batch_step(b->d_members, int(b->members.size()), b->nitems, b->grid,
+                                    parity, b->packed, st);
+  if (e) return e;
+  return launch_batch_monitor(b->d_mons, int(b->members.size()), parity ^ 1, st);
+}
 
 extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, int n, fslbm_batch** out) {
   if (!ctx || !out || n < 1 || !solves) return fslbm_set_error(FSLBM_ERR_ARG, "batch_create: bad argument");
-  auto* b = new fslbm_batch{ctx, {}};
+  auto* b = new fslbm_batch;
+  b->ctx = ctx;
+  bool fast = true;
   for (int i = 0; i < n; ++i) {
     if (!solves[i] || solves[i]->ctx != ctx) {
-      delete b;
+      free_batch(b);
       return fslbm_set_error(FSLBM_ERR_ARG, "batch_create: member %d is null or of another context", i);
     }
     b->members.push_back(solves[i]);
+    fast = fast && solves[i]->use2 && solves[i]->ty2 == 32 && solves[i]->prm.d1 == 2;
+  }
+  b->fast = fast;
+  if (const char* ec = std::getenv("FSLBM_BATCH_CHUNK")) b->chunk = std::max(8, std::atoi(ec));
+  b->packed = solves[0]->packed2;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (!e && fast) e = batch_prepare();
+  if (!e && fast) e = cudaMalloc(&b->d_members, batch_member_bytes() * n);
+  if (!e && fast) e = cudaMalloc(&b->d_mons, sizeof(BatchMon) * n);
+  if (!e) e = cudaEventCreate(&b->ev0);
+  if (!e) e = cudaEventCreate(&b->ev1);
+  if (e) {
+    free_batch(b);
+    return fslbm_set_error(FSLBM_ERR_CUDA, "batch_create: %s", cudaGetErrorString(e));
   }
   *out = b;
   return FSLBM_OK;
 }
 
 extern "C" int fslbm_batch_destroy(fslbm_batch* b) {
-  delete b;
+  free_batch(b);
   return FSLBM_OK;
 }
 
-extern "C" int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int) {
+extern "C" int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int use_graph) {
   if (!b) return fslbm_set_error(FSLBM_ERR_ARG, "batch_step: null batch");
+  if (nsteps < 0) return fslbm_set_error(FSLBM_ERR_ARG, "batch_step: negative step count");
   for (fslbm_solve* s : b->members)
-    if (int r = fslbm_solve_step(s, nsteps)) return r;
+    if (!s->fields_set) return fslbm_set_error(FSLBM_ERR_STATE, "batch_step: a member has no fields");
+  CUDA_TRY(cudaSetDevice(b->ctx->device));
+  cudaStream_t st = b->ctx->stream;
+  if (!b->fast) {
+    CUDA_TRY(cudaEventRecord(b->ev0, st));
+    for (fslbm_solve* s : b->members)
+      if (int r = enqueue_steps(s, nsteps)) return r;
+    CUDA_TRY(cudaEventRecord(b->ev1, st));
+    return FSLBM_OK;
+  }
+  if (int r = batch_upload(b)) return r;
+  CUDA_TRY(cudaEventRecord(b->ev0, st));
+  int64_t left = nsteps;
+  if (use_graph && left >= 2) {
+    if (!b->exec2) {
+      cudaGraph_t graph;
+      CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      cudaError_t e1 = batch_enqueue_one(b, 0, st);
+      cudaError_t e2 = e1 ? e1 : batch_enqueue_one(b, 1, st);
+      cudaError_t e3 = cudaStreamEndCapture(st, &graph);
+      if (e2 || e3)
+        return fslbm_set_error(FSLBM_ERR_CUDA, "batch_step: graph capture: %s",
+                               cudaGetErrorString(e2 ? e2 : e3));
+      cudaError_t e4 = cudaGraphInstantiate(&b->exec2, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e4) return fslbm_set_error(FSLBM_ERR_CUDA, "batch_step: graph instantiate: %s", cudaGetErrorString(e4));
+    }
+    for (; left >= 2; left -= 2) CUDA_TRY(cudaGraphLaunch(b->exec2, st));
+  }
+  int parity = 0;
+  for (; left > 0; --left, parity ^= 1) CUDA_TRY(batch_enqueue_one(b, parity, st));
+  CUDA_TRY(cudaEventRecord(b->ev1, st));
+  for (fslbm_solve* s : b->members) {
+    s->steps += nsteps;
+    s->cur ^= int(nsteps & 1);
+    s->launches += 2 * nsteps;   // counted per member: each batched launch serves all members
+  }
   return FSLBM_OK;
 }
 
 extern "C" int fslbm_batch_sync(fslbm_batch* b) {
   if (!b) return fslbm_set_error(FSLBM_ERR_ARG, "batch_sync: null batch");
-  for (fslbm_solve* s : b->members)
-    if (int r = fslbm_solve_sync(s)) return r;
+  CUDA_TRY(cudaSetDevice(b->ctx->device));
+  CUDA_TRY(cudaStreamSynchronize(b->ctx->stream));
+  elapsed_if_recorded(b->ev0, b->ev1, &b->last_ms);
+  for (fslbm_solve* s : b->members) {
+    unsigned err = 0;
+    CUDA_TRY(cudaMemcpy(&err, s->d_err, sizeof err, cudaMemcpyDeviceToHost));
+    if (err) {
+      cudaMemset(s->d_err, 0, sizeof(unsigned));
+      return fslbm_set_error(FSLBM_ERR_TIMEOUT, "batch_sync: a bounded device wait gave up");
+    }
+  }
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_batch_elapsed(fslbm_batch* b, double* ms) {
+  if (!b || !ms) return fslbm_set_error(FSLBM_ERR_ARG, "batch_elapsed: null argument");
+  *ms = b->last_ms;
   return FSLBM_OK;
 }

@@ -67,6 +67,24 @@ struct MonitorLaunch {
 };
 cudaError_t launch_monitor(const MonitorLaunch& a, cudaStream_t st);
 
+// ---- batched ensemble (FP32 column-pair kernel, d1 = 2, tile height 32)
+struct BatchMon {
+  MonitorLaunch mon;           // state is chosen per launch from `state`
+  const void* state[2];
+  int monitor_every;
+  int cur0;
+};
+cudaError_t batch_prepare();
+size_t batch_member_bytes();
+// Writes one member descriptor (layout private to the kernels) into host memory at dst.
+cudaError_t fill_batch_member(void* dst, const CUtensorMap* map_p, const CUtensorMap* map_u,
+                              const StepLaunch& a, void* state0, void* state1,
+                              const double* gauge_slot, const long long* steps, int monitor_every,
+                              int cur0, int nchunks, int item0);
+cudaError_t launch_batch_step(const void* members, int nmembers, int nitems, int grid, int parity,
+                              int packed, cudaStream_t st);
+cudaError_t launch_batch_monitor(const BatchMon* mons, int n, int parity_after, cudaStream_t st);
+
 cudaError_t launch_zero_walls(int dtype, void* state, const uint8_t* mask, int lxp, int ly, int L,
                               cudaStream_t st);
 cudaError_t launch_plane_stats(int dtype, const void* state, const uint8_t* mask, int lxp, int ly,

@@ -1,6 +1,7 @@
 // Kernel launchers and the small auxiliary kernels of the solve runtime (monitor reduction,
 // statistics accumulation, field conversion, divergence check).
 #include <cstdio>
+#include <cstring>
 #include "internal.h"
 #include "step_kernel.cuh"
 #include "step2_kernel.cuh"
@@ -169,8 +170,7 @@ __device__ void block_sum(double (&v)[NV], double* sh /* NV * 32 */) {
 // monitor (FSLBM.cu:632-666), FP64 sums, one block
 // ------------------------------------------------------------------------------------------
 template <class TS>
-__global__ void monitor_kernel(MonitorLaunch a) {
-  __shared__ double sh[3 * 32];
+__device__ void monitor_body(const MonitorLaunch& a, double* sh) {
   const TS* st = reinterpret_cast<const TS*>(a.state);
   const size_t FS = size_t(a.lxp) * a.ly * a.L;
   const TS pin = TS(a.pin);
@@ -195,6 +195,82 @@ __global__ void monitor_kernel(MonitorLaunch a) {
     a.counters->records = idx + 1;
     *a.gauge_out = p2;
   }
+}
+
+template <class TS>
+__global__ void monitor_kernel(MonitorLaunch a) {
+  __shared__ double sh[3 * 32];
+  monitor_body<TS>(a, sh);
+}
+
+// Batched bookkeeping after a batched step: block i advances member i's step counter and, when
+// the member is due, writes its monitor record and the gauge of its next step.
+__global__ void batch_monitor_kernel(const BatchMon* mons, int parity_after) {
+  __shared__ double sh[3 * 32];
+  __shared__ int due;
+  const BatchMon& b = mons[blockIdx.x];
+  if (threadIdx.x == 0) {
+    const long long s = b.mon.counters->steps + 1;
+    b.mon.counters->steps = s;
+    due = b.monitor_every > 0 && s % b.monitor_every == 0;
+  }
+  __syncthreads();
+  if (!due) return;
+  MonitorLaunch a = b.mon;
+  a.state = b.state[b.cur0 ^ parity_after];
+  monitor_body<float>(a, sh);
+}
+
+cudaError_t launch_batch_monitor(const BatchMon* mons, int n, int parity_after, cudaStream_t st) {
+  batch_monitor_kernel<<<n, 512, 0, st>>>(mons, parity_after);
+  return cudaGetLastError();
+}
+
+template <int TY, bool PK> static cudaError_t batch_prep() {
+  return cudaFuncSetAttribute(fslbm_step2_batch_kernel<2, TY, PK>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(Step2Tile<2, TY>::SMEM_BYTES));
+}
+
+cudaError_t batch_prepare() {
+  cudaError_t e = batch_prep<32, true>();
+  if (e) return e;
+  return batch_prep<32, false>();
+}
+
+size_t batch_member_bytes() { return sizeof(BatchMember); }
+
+cudaError_t fill_batch_member(void* dst, const CUtensorMap* mp, const CUtensorMap* mu,
+                              const StepLaunch& a, void* state0, void* state1,
+                              const double* gauge_slot, const long long* steps, int monitor_every,
+                              int cur0, int nchunks, int item0) {
+  BatchMember m;
+  std::memset(&m, 0, sizeof m);
+  m.map_p[0] = mp[0]; m.map_p[1] = mp[1];
+  m.map_u[0] = mu[0]; m.map_u[1] = mu[1];
+  m.g.lxp = a.lxp; m.g.ly = a.ly; m.g.L = a.L; m.g.ntiles = a.ntiles; m.g.nchunks = nchunks;
+  m.g.tiles = a.tiles; m.g.mask = a.mask; m.g.colcoef = a.colcoef; m.g.out = nullptr;
+  m.g.gauge = nullptr; m.g.err = a.err; m.g.step_counter = nullptr;
+  m.k.tb = float(a.tb); m.k.cc = float(a.cc); m.k.pin = float(a.pin); m.k.dtddy = float(a.dtddy);
+  m.k.m = float(a.m); m.k.c0 = float(a.c0); m.k.c1 = float(a.c1); m.k.c2 = float(a.c2);
+  m.k.fx = float(a.fx); m.k.fy = float(a.fy); m.k.fz = float(a.fz);
+  m.state[0] = state0; m.state[1] = state1;
+  m.gauge_slot = gauge_slot; m.steps = steps; m.monitor_every = monitor_every;
+  m.cur0 = cur0; m.item0 = item0; m.nitems = a.ntiles * nchunks;
+  std::memcpy(dst, &m, sizeof m);
+  return cudaSuccess;
+}
+
+cudaError_t launch_batch_step(const void* members, int nmembers, int nitems, int grid, int parity,
+                              int packed, cudaStream_t st) {
+  const BatchMember* mb = reinterpret_cast<const BatchMember*>(members);
+  if (packed)
+    fslbm_step2_batch_kernel<2, 32, true><<<grid, Step2Tile<2, 32>::THREADS, Step2Tile<2, 32>::SMEM_BYTES, st>>>(
+        mb, nmembers, nitems, parity);
+  else
+    fslbm_step2_batch_kernel<2, 32, false><<<grid, Step2Tile<2, 32>::THREADS, Step2Tile<2, 32>::SMEM_BYTES, st>>>(
+        mb, nmembers, nitems, parity);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_monitor(const MonitorLaunch& a, cudaStream_t st) {

@@ -117,27 +117,26 @@ __device__ __forceinline__ float2 qof(float2 P, float2 U, float2 V, float2 W) {
   return F::fma(f2(-1.5f), F::fma(U, U, F::fma(V, V, F::mul(W, W))), P);
 }
 
+// Marches one (tile, chunk) work item of one pipe: the step of every cell of the tile's columns
+// in the chunk's planes. `reinit` re-arms the CTA's mbarriers when the CTA has marched an item
+// before (persistent grids). Returns false when a bounded wait gave up (error flag set).
 template <int D1, int TY, bool PK>
-__global__ void __launch_bounds__(Step2Tile<D1, TY>::THREADS, 1)
-    fslbm_step2_kernel(const __grid_constant__ CUtensorMap tmap_p,
-                       const __grid_constant__ CUtensorMap tmap_uvw, const Step2Geom g,
-                       const StepConst<float> k) {
+__device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUtensorMap* tmap_uvw,
+                                            const Step2Geom& g, const StepConst<float>& k,
+                                            int tile, int chunk, unsigned char* smem, bool reinit) {
   using Tl = Step2Tile<D1, TY>;
   using F = Pair<PK>;
   static_assert(D1 == 2, "the march prologue below is written for d1 = 2 (R = 4)");
   constexpr int R = Tl::R, HX = Tl::HX, HY = Tl::HY, SW = Tl::SW, S = Tl::S, AH = Tl::AHEAD;
   constexpr int PPL = Tl::PPLANE, UPL = Tl::UPLANE, SLOT = Tl::SLOT;
 
-  extern __shared__ __align__(128) unsigned char smem[];
   float* ring = reinterpret_cast<float*>(smem);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + Tl::BAR_OFFSET);
   uint64_t* empty = full + S;
 
   const int tid = threadIdx.x, lane = tid & 31, tp = tid % (Tl::TX / 2), ty = tid / (Tl::TX / 2);
-  if (tid == 0 && blockIdx.x == 0 && g.step_counter) *g.step_counter += 1;
 
   // ---- work: one (tile, chunk); odd chunks march towards -z
-  const int tile = blockIdx.x % g.ntiles, chunk = blockIdx.x / g.ntiles;
   const int zb = int((long long)g.L * chunk / g.nchunks);
   const int ze = int((long long)g.L * (chunk + 1) / g.nchunks);
   const int dir = (chunk & 1) ? -1 : 1;
@@ -156,8 +155,10 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY>::THREADS, 1)
   }
   const bool warp_on = __any_sync(0xffffffffu, fl.x != 0.f || fl.y != 0.f);
 
+  __syncthreads();   // a previous item (persistent grids) is fully consumed
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
+      if (reinit) { mbar_inval(&full[s]); mbar_inval(&empty[s]); }
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], Tl::WARPS);
     }
@@ -171,13 +172,13 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY>::THREADS, 1)
     if (zz < 0) zz += g.L;
     float* dst = ring + slot * SLOT;
     mbar_arrive_expect_tx(&full[slot], Tl::TX_BYTES);
-    tma_load_4d(dst, &tmap_p, &full[slot], org.x - HX, org.y - 1, zz, 0);
-    tma_load_4d(dst + PPL, &tmap_uvw, &full[slot], org.x - HX, org.y - HY, zz, 1);
+    tma_load_4d(dst, tmap_p, &full[slot], org.x - HX, org.y - 1, zz, 0);
+    tma_load_4d(dst + PPL, tmap_uvw, &full[slot], org.x - HX, org.y - HY, zz, 1);
   };
   int issued = -1;                                            // last march plane issued (thread 0)
   if (tid == 0) {
-    prefetch_tensormap(&tmap_p);
-    prefetch_tensormap(&tmap_uvw);
+    prefetch_tensormap(tmap_p);
+    prefetch_tensormap(tmap_uvw);
     for (int m = 0; m <= AH && m < niter; ++m) { issue(m); issued = m; }
   }
   auto drain = [&](int from) {                                // failure path: let loads land
@@ -213,8 +214,8 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY>::THREADS, 1)
 
   if (!warp_on) {   // all-wall warps keep the pipeline protocol only
     for (int m = 0; m < niter; ++m)
-      if (!arrive_wait(m) || !release_produce(m)) return;
-    return;
+      if (!arrive_wait(m) || !release_produce(m)) return false;
+    return true;
   }
 
   const float gauge = g.gauge ? float(*g.gauge) : 0.0f;
@@ -392,7 +393,7 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY>::THREADS, 1)
   // predictor sums of the first output
 #pragma unroll
   for (int m = 0; m < 2 * R; ++m) {
-    if (!arrive_wait(m)) return;
+    if (!arrive_wait(m)) return false;
     if (m >= 2 * R - 2) predictor(m - R + 1);
     if (m >= R) {
       float2 uc, vc, wc;
@@ -403,29 +404,82 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY>::THREADS, 1)
       else if (h == 2) { hu[2] = uc; hv[2] = vc; hw[2] = wc; }
       else { hu[3] = uc; hv[3] = vc; hw[3] = wc; }
     }
-    if (!release_produce(m)) return;
+    if (!release_produce(m)) return false;
   }
   // ---- steady state, four planes per pass (the history period)
   for (int m = 2 * R; m < niter; m += 4) {
-    if (!arrive_wait(m)) return;
+    if (!arrive_wait(m)) return false;
     predictor(m - R + 1);
     output(m - R, I0{});
-    if (!release_produce(m)) return;
+    if (!release_produce(m)) return false;
     if (m + 1 >= niter) break;
-    if (!arrive_wait(m + 1)) return;
+    if (!arrive_wait(m + 1)) return false;
     predictor(m - R + 2);
     output(m - R + 1, I1{});
-    if (!release_produce(m + 1)) return;
+    if (!release_produce(m + 1)) return false;
     if (m + 2 >= niter) break;
-    if (!arrive_wait(m + 2)) return;
+    if (!arrive_wait(m + 2)) return false;
     predictor(m - R + 3);
     output(m - R + 2, I2{});
-    if (!release_produce(m + 2)) return;
+    if (!release_produce(m + 2)) return false;
     if (m + 3 >= niter) break;
-    if (!arrive_wait(m + 3)) return;
+    if (!arrive_wait(m + 3)) return false;
     predictor(m - R + 4);
     output(m - R + 3, I3{});
-    if (!release_produce(m + 3)) return;
+    if (!release_produce(m + 3)) return false;
+  }
+  return true;
+}
+
+// One pipe, one step: CTA b marches (tile b % ntiles, chunk b / ntiles).
+template <int D1, int TY, bool PK>
+__global__ void __launch_bounds__(Step2Tile<D1, TY>::THREADS, 1)
+    fslbm_step2_kernel(const __grid_constant__ CUtensorMap tmap_p,
+                       const __grid_constant__ CUtensorMap tmap_uvw, const Step2Geom g,
+                       const StepConst<float> k) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  if (threadIdx.x == 0 && blockIdx.x == 0 && g.step_counter) *g.step_counter += 1;
+  step2_march<D1, TY, PK>(&tmap_p, &tmap_uvw, g, k, blockIdx.x % g.ntiles,
+                          blockIdx.x / g.ntiles, smem, false);
+}
+
+// One member of a batched ensemble: its tensor maps for both state buffers, its step geometry
+// and constants, and its share of the work items.
+struct alignas(64) BatchMember {
+  CUtensorMap map_p[2], map_u[2];
+  Step2Geom g;                 // g.out is replaced by the buffer the step writes
+  StepConst<float> k;
+  void* state[2];
+  const double* gauge_slot;    // the member's monitor p2, applied on the step after a monitor
+  const long long* steps;      // the member's device step counter
+  int monitor_every;
+  int cur0;                    // input buffer at batch parity 0
+  int item0, nitems;           // first work item and item count (tiles x chunks)
+};
+
+// Many pipes, one step each: a persistent grid walks the work items of all members.
+template <int D1, int TY, bool PK>
+__global__ void __launch_bounds__(Step2Tile<D1, TY>::THREADS, 1)
+    fslbm_step2_batch_kernel(const BatchMember* __restrict__ members, int nmembers, int nitems,
+                             int parity) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  int mi = 0;
+  bool first = true;
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    while (mi + 1 < nmembers && members[mi + 1].item0 <= item) ++mi;
+    const BatchMember& mb = members[mi];
+    const int cur = mb.cur0 ^ parity;
+    Step2Geom g = mb.g;
+    g.out = mb.state[1 - cur];
+    g.step_counter = nullptr;
+    const long long done = *mb.steps;
+    g.gauge = (mb.monitor_every > 0 && done > 0 && done % mb.monitor_every == 0) ? mb.gauge_slot
+                                                                              : nullptr;
+    const int local = item - mb.item0;
+    if (!step2_march<D1, TY, PK>(&mb.map_p[cur], &mb.map_u[cur], g, mb.k, local % g.ntiles,
+                                 local / g.ntiles, smem, !first))
+      return;
+    first = false;
   }
 }
 

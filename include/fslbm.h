@@ -169,9 +169,14 @@ int fslbm_profile_reset(fslbm_solve* s);
 /* ---- batched ensemble: many solves advanced by one persistent launch per step group ---- */
 int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, int n, fslbm_batch** out);
 int fslbm_batch_destroy(fslbm_batch* b);
-/* Advances every member nsteps steps; with use_graph the step group is a captured CUDA graph. */
+/* Advances every member nsteps steps, asynchronously. When every member is FP32 with d1 = 2, a
+ * time step of the whole ensemble is one persistent launch over all members' (tile, chunk) work
+ * items plus one bookkeeping launch (step counters, monitors, gauges); with use_graph two such
+ * steps are replayed from a captured CUDA graph. Other members step one after another. */
 int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int use_graph);
 int fslbm_batch_sync(fslbm_batch* b);
+/* Device time of the last fslbm_batch_step call (valid after fslbm_batch_sync). */
+int fslbm_batch_elapsed(fslbm_batch* b, double* ms);
 
 /* ---- allocation-free step ---- */
 /* No counterpart in the reference. Advances a caller-owned FP32 state by one step (the same

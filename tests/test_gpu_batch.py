@@ -1,0 +1,73 @@
+"""Batched ensemble: members of uneven size advanced together (one persistent launch per time
+step, CUDA graph replay) must give each member's own plain-path result. The batched launch
+chooses its own streamwise chunking, so planes may be marched in the other direction than on
+the plain path; the tolerance is FP32 reassociation level, 1e-6 relative L2 per member, and
+monitor records agree to 1e-5 relative (pressure means on the scale u_b^2)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def member_specs(n=6, seed=4):
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n):
+        ny = int(rng.integers(24, 70))
+        L = int(rng.integers(32, 140))
+        R = ny / 2 - 1
+        re = float(np.exp(rng.uniform(np.log(50), np.log(3000))))
+        ub = 0.1
+        nu = 2 * R * ub / re
+        g = 8 * nu * ub / R ** 2
+        specs.append(dict(lx=ny, ly=ny, L=L, R=R, nu=nu, g=g, ub=ub, seed=100 + i))
+    return specs
+
+
+def make_member(fb, ctx, sp, monitor_every=25):
+    c = (sp["lx"] - 1) / 2
+    dom = fb.make_domain(sp["lx"], sp["ly"], sp["L"], radius=sp["R"], cx=c, cy=c)
+    prm = fb.Params.make(tblend=0.5, pin=0.0, nu=sp["nu"], d1=2, delta=1, blend=1.0,
+                         monitor_every=monitor_every, force=(0.0, 0.0, -sp["g"]))
+    s = fb.Solve(ctx, dom, prm, fb.F32)
+    f = fb.init_poiseuille(dom, 2 * sp["ub"], noise=0.02, modes=2, mode_amp=0.05, seed=sp["seed"])
+    s.set_fields(f)
+    return s
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_batch_matches_members_alone(built, ctx, use_graph):
+    fb = built
+    specs = member_specs()
+    steps = 61   # odd: graph pairs plus one direct step
+    alone = []
+    for sp in specs:
+        s = make_member(fb, ctx, sp)
+        s.step(steps)
+        s.sync()
+        alone.append((s.get_fields(np.float32), s.monitor_log()))
+        s.close()
+    members = [make_member(fb, ctx, sp) for sp in specs]
+    b = fb.Batch(ctx, members)
+    b.step(steps, use_graph=use_graph)
+    b.sync()
+    assert b.elapsed_ms() > 0
+    for s, (want, wlog) in zip(members, alone):
+        got = s.get_fields(np.float32)
+        err = np.linalg.norm((got - want).astype(np.float64)) / np.linalg.norm(want.astype(np.float64))
+        assert err <= 1e-6, err
+        assert s.info()["steps"] == steps
+        glog = s.monitor_log()
+        assert [r["step"] for r in glog] == [r["step"] for r in wlog] == [25, 50]
+        # means of pressure cancel to ~1e-5; compare them on the scale of u_b^2 = 1e-2
+        for r, w in zip(glog, wlog):
+            for key, scale in (("q1", 0.0), ("p1", 1e-2), ("p2", 1e-2), ("sample", 0.0)):
+                tol = 1e-5 * max(abs(w[key]), scale, 1e-6)
+                assert abs(r[key] - w[key]) <= tol, (key, r[key], w[key])
+    # members stay usable on their own after batched steps
+    members[0].step(3)
+    members[0].sync()
+    assert members[0].info()["steps"] == steps + 3
+    b.close()
+    for s in members:
+        s.close()
