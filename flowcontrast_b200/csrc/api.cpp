@@ -187,25 +187,28 @@ static int validate_params(const fslbm_params* p, int dtype) {
 static int build_tensor_maps(fslbm_solve* s) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return fslbm_set_error(FSLBM_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
-  int sw, sh, hx, hy;
-  if (!step_box(s->dtype, s->prm.d1, &sw, &sh, &hx, &hy))
-    return fslbm_set_error(FSLBM_ERR_ARG, "no step kernel for dtype %d d1 %d", s->dtype, s->prm.d1);
-  const CUtensorMapDataType dt =
-      s->dtype == FSLBM_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const CUtensorMapDataType dt = s->dtype == FSLBM_F64   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                 : s->dtype == FSLBM_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   for (int b = 0; b < 2; ++b) {
     cuuint64_t dims[4] = {cuuint64_t(s->lxp), cuuint64_t(s->ly), cuuint64_t(s->L), 4};
     cuuint64_t strides[3] = {cuuint64_t(s->lxp) * s->es, cuuint64_t(s->lxp) * s->ly * s->es,
                              cuuint64_t(field_stride(s)) * s->es};
-    cuuint32_t box[4] = {cuuint32_t(sw), cuuint32_t(sh), 1, 4};
     cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = enc(&s->maps[b], dt, 4, s->state[b], dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS)
-      return fslbm_set_error(FSLBM_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
-    if (s->use2) {
+    CUresult r;
+    if (!s->use2) {
+      int sw, sh, hx, hy;
+      if (!step_box(s->dtype, s->prm.d1, &sw, &sh, &hx, &hy))
+        return fslbm_set_error(FSLBM_ERR_ARG, "no step kernel for dtype %d d1 %d", s->dtype, s->prm.d1);
+      cuuint32_t box[4] = {cuuint32_t(sw), cuuint32_t(sh), 1, 4};
+      r = enc(&s->maps[b], dt, 4, s->state[b], dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS)
+        return fslbm_set_error(FSLBM_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
+    } else {
       int sw2, ph, uh, hx2, hy2;
-      if (!step2_box(s->prm.d1, s->ty2, &sw2, &ph, &uh, &hx2, &hy2))
+      if (!step2_box(s->dtype, s->prm.d1, s->ty2, &sw2, &ph, &uh, &hx2, &hy2))
         return fslbm_set_error(FSLBM_ERR_ARG, "no column-pair kernel for d1 %d", s->prm.d1);
       cuuint32_t boxp[4] = {cuuint32_t(sw2), cuuint32_t(ph), 1, 1};
       cuuint32_t boxu[4] = {cuuint32_t(sw2), cuuint32_t(uh), 1, 3};
@@ -245,7 +248,9 @@ static void choose_chunks(fslbm_solve* s);
 static int configure_kernel(fslbm_solve* s) {
   const char* ek = std::getenv("FSLBM_STEP_KERNEL");
   const char* et = std::getenv("FSLBM_TILE_Y");
-  s->use2 = step2_supported(s->dtype, s->prm.d1) && !(ek && std::atoi(ek) == 1);
+  // FP16 storage exists only in the column-pair kernel
+  s->use2 = step2_supported(s->dtype, s->prm.d1) &&
+            (s->dtype == FSLBM_F16 || !(ek && std::atoi(ek) == 1));
   s->ty2 = (et && std::atoi(et) == 16) ? 16 : 32;
   const char* ep = std::getenv("FSLBM_PACKED");
   s->packed2 = (ep && std::atoi(ep) == 0) ? 0 : 1;
@@ -260,7 +265,7 @@ static int configure_kernel(fslbm_solve* s) {
   s->bytes_device += int64_t(tiles.size() * sizeof(int2));
   CUDA_TRY(cudaMemcpy(s->d_tiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice));
   if (s->use2) {
-    CUDA_TRY(step2_prepare(s->prm.d1, s->ty2));
+    CUDA_TRY(step2_prepare(s->dtype, s->prm.d1, s->ty2));
     // tiles x streamwise chunks, at most one CTA per SM slot and chunks of at least 2R planes
     const int slots = s->ctx->sm_count * step2_occupancy(s->prm.d1, s->ty2);
     int nch = std::max(1, slots / s->ntiles);
@@ -345,7 +350,7 @@ static cudaError_t dalloc(fslbm_solve* s, T** p, size_t bytes) {
 extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const fslbm_params* prm,
                                   fslbm_dtype dtype, fslbm_solve** out) {
   if (!ctx || !dom || !out) return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: null argument");
-  if (dtype != FSLBM_F32 && dtype != FSLBM_F64)
+  if (dtype != FSLBM_F32 && dtype != FSLBM_F64 && dtype != FSLBM_F16)
     return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: dtype %d is not available", int(dtype));
   int rc = validate_params(prm, dtype);
   if (rc) return rc;
@@ -365,7 +370,7 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
   s->lxp = (dom->lx + 7) / 8 * 8;
   s->d2 = dom->buffer_depth;
   s->dtype = dtype;
-  s->es = dtype == FSLBM_F64 ? 8 : 4;
+  s->es = dtype == FSLBM_F64 ? 8 : (dtype == FSLBM_F16 ? 2 : 4);
   s->prm = *prm;
   s->mask.assign(size_t(s->lxp) * s->ly, kWall);
   double sxs = 0, sys = 0;
@@ -537,11 +542,11 @@ extern "C" int fslbm_solve_get_fields(fslbm_solve* s, fslbm_dtype hd, void* p, v
   return FSLBM_OK;
 }
 
-// Per-step constants formed as the reference forms them (FSLBM.cu:231, 269, 599, 624): in the
-// storage precision for FP32, in FP64 otherwise.
+// Per-step constants formed as the reference forms them (FSLBM.cu:231, 269, 599, 624): in FP32
+// for the FP32-arithmetic forms (FP32 and FP16 storage), in FP64 otherwise.
 static void fill_constants(const fslbm_solve* s, StepLaunch& a) {
   const fslbm_params& p = s->prm;
-  if (s->dtype == FSLBM_F32) {
+  if (s->dtype != FSLBM_F64) {
     const float tb = float(p.tblend), nu = float(p.nu), blend = float(p.blend);
     a.tb = tb;
     a.cc = float(1.0 - double(tb));
@@ -577,7 +582,7 @@ static int enqueue_steps(fslbm_solve* s, int64_t nsteps) {
   MonitorLaunch m{};
   m.dtype = s->dtype; m.mask = s->d_mask;
   m.lxp = s->lxp; m.lx = s->lx; m.ly = s->ly; m.L = s->L;
-  m.pin = s->dtype == FSLBM_F32 ? double(float(s->prm.pin)) : s->prm.pin;
+  m.pin = s->dtype != FSLBM_F64 ? double(float(s->prm.pin)) : s->prm.pin;
   m.nu = s->prm.nu; m.radius = s->radius; m.l1 = double(s->fluid2d);
   m.sx = s->sx; m.sy = s->sy; m.sz = s->sz;
   m.log = s->d_log; m.log_cap = s->log_cap; m.gauge_out = s->d_gauge; m.counters = s->d_counters;
@@ -586,6 +591,7 @@ static int enqueue_steps(fslbm_solve* s, int64_t nsteps) {
     const int64_t c = s->steps + 1;
     a.map = &s->maps[s->cur];
     a.out = s->state[1 - s->cur];
+    a.step_no = c;
     a.gauge = (me > 0 && c > 1 && (c - 1) % me == 0) ? s->d_gauge : nullptr;
     if (s->timing) {
       while (s->tev.size() < s->tev_used + 2) {
@@ -842,7 +848,7 @@ extern "C" int fslbm_stats_sample(fslbm_solve* s) {
     CUDA_TRY(cudaMemsetAsync(s->d_stats + 4 * n, 0, 7 * n * sizeof(double), st));
   }
   s->cnt += 1; s->cnt2 += 1;                                   // FSLBM.cu:715
-  const double pin = s->dtype == FSLBM_F32 ? double(float(s->prm.pin)) : s->prm.pin;
+  const double pin = s->dtype != FSLBM_F64 ? double(float(s->prm.pin)) : s->prm.pin;
   CUDA_TRY(launch_plane_stats(s->dtype, s->state[s->cur], s->d_mask, s->lxp, s->ly, s->L, s->d2,
                               s->lx / 2, pin, s->cnt, 1, 1, s->d_stats, st));
   return FSLBM_OK;
@@ -989,7 +995,7 @@ static int batch_upload(fslbm_batch* b) {
 }
 
 static cudaError_t batch_enqueue_one(fslbm_batch* b, int parity, cudaStream_t st) {
-  cudaError_t e = launch_batch_step(b->d_members, int(b->members.size()), b->nitems, b->grid,
+  cudaError_t e = launch_batch_step(b->members[0]->dtype, b->d_members, int(b->members.size()), b->nitems, b->grid,
                                     parity, b->packed, st);
   if (e) return e;
   return launch_batch_monitor(b->d_mons, int(b->members.size()), parity ^ 1, st);
@@ -1006,13 +1012,14 @@ extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, in
       return fslbm_set_error(FSLBM_ERR_ARG, "batch_create: member %d is null or of another context", i);
     }
     b->members.push_back(solves[i]);
-    fast = fast && solves[i]->use2 && solves[i]->ty2 == 32 && solves[i]->prm.d1 == 2;
+    fast = fast && solves[i]->use2 && solves[i]->ty2 == 32 && solves[i]->prm.d1 == 2 &&
+           solves[i]->dtype == solves[0]->dtype;
   }
   b->fast = fast;
   if (const char* ec = std::getenv("FSLBM_BATCH_CHUNK")) b->chunk = std::max(8, std::atoi(ec));
   b->packed = solves[0]->packed2;
   cudaError_t e = cudaSetDevice(ctx->device);
-  if (!e && fast) e = batch_prepare();
+  if (!e && fast) e = batch_prepare(solves[0]->dtype);
   if (!e && fast) e = cudaMalloc(&b->d_members, batch_member_bytes() * n);
   if (!e && fast) e = cudaMalloc(&b->d_mons, sizeof(BatchMon) * n);
   if (!e) e = cudaEventCreate(&b->ev0);

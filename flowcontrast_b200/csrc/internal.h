@@ -29,6 +29,7 @@ struct StepLaunch {
   const double* gauge;
   unsigned* err;
   DevCounters* counters;     // steps incremented by the launch
+  long long step_no;         // the time step this launch computes (1-based; rounding seed)
   // constants in double; converted to the compute type by the launcher
   double tb, cc, pin, dtddy, m, c0, c1, c2, fx, fy, fz;
 };
@@ -48,9 +49,9 @@ struct Step2Launch {
   int grid;
 };
 bool step2_supported(int dtype, int d1);
-bool step2_box(int d1, int ty, int* sw, int* ph, int* uh, int* hx, int* hy);
+bool step2_box(int dtype, int d1, int ty, int* sw, int* ph, int* uh, int* hx, int* hy);
 int step2_occupancy(int d1, int ty);   // CTAs per SM the kernel is built for
-cudaError_t step2_prepare(int d1, int ty);
+cudaError_t step2_prepare(int dtype, int d1, int ty);
 cudaError_t launch_step2(const StepLaunch& a, const Step2Launch& b, cudaStream_t st);
 
 struct MonitorLaunch {
@@ -74,14 +75,14 @@ struct BatchMon {
   int monitor_every;
   int cur0;
 };
-cudaError_t batch_prepare();
+cudaError_t batch_prepare(int dtype);
 size_t batch_member_bytes();
 // Writes one member descriptor (layout private to the kernels) into host memory at dst.
 cudaError_t fill_batch_member(void* dst, const CUtensorMap* map_p, const CUtensorMap* map_u,
                               const StepLaunch& a, void* state0, void* state1,
                               const double* gauge_slot, const long long* steps, int monitor_every,
                               int cur0, int nchunks, int item0);
-cudaError_t launch_batch_step(const void* members, int nmembers, int nitems, int grid, int parity,
+cudaError_t launch_batch_step(int dtype, const void* members, int nmembers, int nitems, int grid, int parity,
                               int packed, cudaStream_t st);
 cudaError_t launch_batch_monitor(const BatchMon* mons, int n, int parity_after, cudaStream_t st);
 

@@ -8,6 +8,13 @@
 
 namespace fslbm {
 
+// Arithmetic type of the auxiliary kernels for a storage type (FP16 storage is read as FP32).
+template <class T> struct ArithOf { using type = T; };
+template <> struct ArithOf<__half> { using type = float; };
+__device__ __forceinline__ double to_d(float x) { return double(x); }
+__device__ __forceinline__ double to_d(double x) { return x; }
+__device__ __forceinline__ double to_d(__half x) { return double(__half2float(x)); }
+
 // ------------------------------------------------------------------------------------------
 // step dispatch
 // ------------------------------------------------------------------------------------------
@@ -42,6 +49,7 @@ template <class TS, int D1> static size_t smem_t() { return StepTile<TS, D1>::SM
 bool step_supported(int dtype, int d1) {
   if (dtype == FSLBM_F32) return d1 >= 1 && d1 <= 3;
   if (dtype == FSLBM_F64) return d1 >= 1 && d1 <= 2;
+  if (dtype == FSLBM_F16) return d1 == 2;      // column-pair kernel only
   return false;
 }
 
@@ -84,40 +92,72 @@ cudaError_t launch_step(const StepLaunch& a, cudaStream_t st) {
 // ------------------------------------------------------------------------------------------
 // FP32 column-pair kernel dispatch
 // ------------------------------------------------------------------------------------------
-bool step2_supported(int dtype, int d1) { return dtype == FSLBM_F32 && d1 == 2; }
+bool step2_supported(int dtype, int d1) {
+  return (dtype == FSLBM_F32 || dtype == FSLBM_F16) && d1 == 2;
+}
 
-template <int TY> static void box2(int* sw, int* ph, int* uh, int* hx, int* hy) {
-  using Tl = Step2Tile<2, TY>;
+template <int TY, class TE> static void box2(int* sw, int* ph, int* uh, int* hx, int* hy) {
+  using Tl = Step2Tile<2, TY, TE>;
   *sw = Tl::SW; *ph = Tl::PH; *uh = Tl::UH; *hx = Tl::HX; *hy = Tl::HY;
 }
 
-bool step2_box(int d1, int ty, int* sw, int* ph, int* uh, int* hx, int* hy) {
-  if (d1 != 2) return false;
-  if (ty == 32) { box2<32>(sw, ph, uh, hx, hy); return true; }
-  if (ty == 16) { box2<16>(sw, ph, uh, hx, hy); return true; }
+bool step2_box(int dtype, int d1, int ty, int* sw, int* ph, int* uh, int* hx, int* hy) {
+  if (d1 != 2 || (ty != 32 && ty != 16)) return false;
+  if (dtype == FSLBM_F32) {
+    if (ty == 32) box2<32, float>(sw, ph, uh, hx, hy);
+    else box2<16, float>(sw, ph, uh, hx, hy);
+    return true;
+  }
+  if (dtype == FSLBM_F16) {
+    if (ty == 32) box2<32, __half>(sw, ph, uh, hx, hy);
+    else box2<16, __half>(sw, ph, uh, hx, hy);
+    return true;
+  }
   return false;
 }
 
 int step2_occupancy(int, int) { return 1; }
 
-template <int TY, bool PK> static cudaError_t prep2() {
-  return cudaFuncSetAttribute(fslbm_step2_kernel<2, TY, PK>,
+template <int TY, bool PK, class TE> static cudaError_t prep2() {
+  return cudaFuncSetAttribute(fslbm_step2_kernel<2, TY, PK, TE>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(Step2Tile<2, TY>::SMEM_BYTES));
+                              int(Step2Tile<2, TY, TE>::SMEM_BYTES));
 }
 
-cudaError_t step2_prepare(int d1, int ty) {
-  if (d1 != 2) return cudaErrorInvalidValue;
+template <class TE> static cudaError_t prep2_all(int ty) {
   cudaError_t e;
   if (ty == 32) {
-    if ((e = prep2<32, true>())) return e;
-    return prep2<32, false>();
+    if ((e = prep2<32, true, TE>())) return e;
+    return prep2<32, false, TE>();
   }
   if (ty == 16) {
-    if ((e = prep2<16, true>())) return e;
-    return prep2<16, false>();
+    if ((e = prep2<16, true, TE>())) return e;
+    return prep2<16, false, TE>();
   }
   return cudaErrorInvalidValue;
+}
+
+cudaError_t step2_prepare(int dtype, int d1, int ty) {
+  if (d1 != 2) return cudaErrorInvalidValue;
+  if (dtype == FSLBM_F32) return prep2_all<float>(ty);
+  if (dtype == FSLBM_F16) return prep2_all<__half>(ty);
+  return cudaErrorInvalidValue;
+}
+
+template <class TE>
+static cudaError_t launch_step2_t(const Step2Launch& b, const Step2Geom& g,
+                                  const StepConst<float>& k, cudaStream_t st) {
+#define FSLBM_L2(TY, PK)                                                                  \
+  fslbm_step2_kernel<2, TY, PK, TE><<<b.grid, Step2Tile<2, TY, TE>::THREADS,              \
+                                      Step2Tile<2, TY, TE>::SMEM_BYTES, st>>>(*b.map_p,  \
+                                                                          *b.map_uvw, g, k)
+  if (b.ty == 32 && b.packed) FSLBM_L2(32, true);
+  else if (b.ty == 32) FSLBM_L2(32, false);
+  else if (b.ty == 16 && b.packed) FSLBM_L2(16, true);
+  else if (b.ty == 16) FSLBM_L2(16, false);
+  else return cudaErrorInvalidValue;
+#undef FSLBM_L2
+  return cudaGetLastError();
 }
 
 cudaError_t launch_step2(const StepLaunch& a, const Step2Launch& b, cudaStream_t st) {
@@ -126,21 +166,15 @@ cudaError_t launch_step2(const StepLaunch& a, const Step2Launch& b, cudaStream_t
   g.tiles = a.tiles; g.mask = a.mask; g.colcoef = a.colcoef; g.out = a.out;
   g.gauge = a.gauge; g.err = a.err;
   g.step_counter = a.counters ? &a.counters->steps : nullptr;
+  g.step_no = unsigned(a.step_no);
   StepConst<float> k;
   k.tb = float(a.tb); k.cc = float(a.cc); k.pin = float(a.pin); k.dtddy = float(a.dtddy);
   k.m = float(a.m); k.c0 = float(a.c0); k.c1 = float(a.c1); k.c2 = float(a.c2);
   k.fx = float(a.fx); k.fy = float(a.fy); k.fz = float(a.fz);
-#define FSLBM_L2(TY, PK)                                                                        \
-  fslbm_step2_kernel<2, TY, PK><<<b.grid, Step2Tile<2, TY>::THREADS, Step2Tile<2, TY>::SMEM_BYTES, \
-                                  st>>>(*b.map_p, *b.map_uvw, g, k)
   if (b.d1 != 2) return cudaErrorInvalidValue;
-  if (b.ty == 32 && b.packed) FSLBM_L2(32, true);
-  else if (b.ty == 32) FSLBM_L2(32, false);
-  else if (b.ty == 16 && b.packed) FSLBM_L2(16, true);
-  else if (b.ty == 16) FSLBM_L2(16, false);
-  else return cudaErrorInvalidValue;
-#undef FSLBM_L2
-  return cudaGetLastError();
+  if (a.dtype == FSLBM_F32) return launch_step2_t<float>(b, g, k, st);
+  if (a.dtype == FSLBM_F16) return launch_step2_t<__half>(b, g, k, st);
+  return cudaErrorInvalidValue;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -171,15 +205,16 @@ __device__ void block_sum(double (&v)[NV], double* sh /* NV * 32 */) {
 // ------------------------------------------------------------------------------------------
 template <class TS>
 __device__ void monitor_body(const MonitorLaunch& a, double* sh) {
+  using TA = typename ArithOf<TS>::type;
   const TS* st = reinterpret_cast<const TS*>(a.state);
   const size_t FS = size_t(a.lxp) * a.ly * a.L;
-  const TS pin = TS(a.pin);
+  const TA pin = TA(a.pin);
   double v[3] = {0, 0, 0};   // sum w, sum p, sum (p - pin) over non-wall cells of plane z=0
   for (int j = threadIdx.x; j < a.lxp * a.ly; j += blockDim.x) {
-    const TS p = st[j];
-    v[0] += double(st[3 * FS + j]);
+    const TA p = TA(st[j]);
+    v[0] += to_d(st[3 * FS + j]);
     v[1] += double(p);
-    if (a.mask[j] != kWall) v[2] += double(TS(p - pin));   // the outlet buffer copy's p
+    if (a.mask[j] != kWall) v[2] += double(TA(p - pin));   // the outlet buffer copy's p
   }
   block_sum<3>(v, sh);
   if (threadIdx.x == 0) {
@@ -188,7 +223,7 @@ __device__ void monitor_body(const MonitorLaunch& a, double* sh) {
     r.step = a.counters->steps;
     r.q1 = q1; r.q2 = q1; r.p1 = p1; r.p2 = p2;
     r.f = (p1 - p2) / q1 / q1 / 3.0 * 4.0 * a.radius / double(a.L);
-    r.sample = double(st[3 * FS + (size_t(a.sz) * a.ly + a.sy) * a.lxp + a.sx]);
+    r.sample = to_d(st[3 * FS + (size_t(a.sz) * a.ly + a.sy) * a.lxp + a.sx]);
     r.re = 2.0 * a.radius * q1 / a.nu;
     const long long idx = a.counters->records;
     a.log[idx % a.log_cap] = r;
@@ -218,7 +253,8 @@ __global__ void batch_monitor_kernel(const BatchMon* mons, int parity_after) {
   if (!due) return;
   MonitorLaunch a = b.mon;
   a.state = b.state[b.cur0 ^ parity_after];
-  monitor_body<float>(a, sh);
+  if (a.dtype == FSLBM_F16) monitor_body<__half>(a, sh);
+  else monitor_body<float>(a, sh);
 }
 
 cudaError_t launch_batch_monitor(const BatchMon* mons, int n, int parity_after, cudaStream_t st) {
@@ -226,16 +262,23 @@ cudaError_t launch_batch_monitor(const BatchMon* mons, int n, int parity_after, 
   return cudaGetLastError();
 }
 
-template <int TY, bool PK> static cudaError_t batch_prep() {
-  return cudaFuncSetAttribute(fslbm_step2_batch_kernel<2, TY, PK>,
+template <bool PK, class TE> static cudaError_t batch_prep() {
+  return cudaFuncSetAttribute(fslbm_step2_batch_kernel<2, 32, PK, TE>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(Step2Tile<2, TY>::SMEM_BYTES));
+                              int(Step2Tile<2, 32, TE>::SMEM_BYTES));
 }
 
-cudaError_t batch_prepare() {
-  cudaError_t e = batch_prep<32, true>();
-  if (e) return e;
-  return batch_prep<32, false>();
+cudaError_t batch_prepare(int dtype) {
+  cudaError_t e;
+  if (dtype == FSLBM_F32) {
+    if ((e = batch_prep<true, float>())) return e;
+    return batch_prep<false, float>();
+  }
+  if (dtype == FSLBM_F16) {
+    if ((e = batch_prep<true, __half>())) return e;
+    return batch_prep<false, __half>();
+  }
+  return cudaErrorInvalidValue;
 }
 
 size_t batch_member_bytes() { return sizeof(BatchMember); }
@@ -250,7 +293,7 @@ cudaError_t fill_batch_member(void* dst, const CUtensorMap* mp, const CUtensorMa
   m.map_u[0] = mu[0]; m.map_u[1] = mu[1];
   m.g.lxp = a.lxp; m.g.ly = a.ly; m.g.L = a.L; m.g.ntiles = a.ntiles; m.g.nchunks = nchunks;
   m.g.tiles = a.tiles; m.g.mask = a.mask; m.g.colcoef = a.colcoef; m.g.out = nullptr;
-  m.g.gauge = nullptr; m.g.err = a.err; m.g.step_counter = nullptr;
+  m.g.gauge = nullptr; m.g.err = a.err; m.g.step_counter = nullptr; m.g.step_no = 0;
   m.k.tb = float(a.tb); m.k.cc = float(a.cc); m.k.pin = float(a.pin); m.k.dtddy = float(a.dtddy);
   m.k.m = float(a.m); m.k.c0 = float(a.c0); m.k.c1 = float(a.c1); m.k.c2 = float(a.c2);
   m.k.fx = float(a.fx); m.k.fy = float(a.fy); m.k.fz = float(a.fz);
@@ -261,21 +304,31 @@ cudaError_t fill_batch_member(void* dst, const CUtensorMap* mp, const CUtensorMa
   return cudaSuccess;
 }
 
-cudaError_t launch_batch_step(const void* members, int nmembers, int nitems, int grid, int parity,
-                              int packed, cudaStream_t st) {
-  const BatchMember* mb = reinterpret_cast<const BatchMember*>(members);
+template <class TE>
+static void launch_batch_t(const BatchMember* mb, int nmembers, int nitems, int grid, int parity,
+                           int packed, cudaStream_t st) {
+  using Tl = Step2Tile<2, 32, TE>;
   if (packed)
-    fslbm_step2_batch_kernel<2, 32, true><<<grid, Step2Tile<2, 32>::THREADS, Step2Tile<2, 32>::SMEM_BYTES, st>>>(
+    fslbm_step2_batch_kernel<2, 32, true, TE><<<grid, Tl::THREADS, Tl::SMEM_BYTES, st>>>(
         mb, nmembers, nitems, parity);
   else
-    fslbm_step2_batch_kernel<2, 32, false><<<grid, Step2Tile<2, 32>::THREADS, Step2Tile<2, 32>::SMEM_BYTES, st>>>(
+    fslbm_step2_batch_kernel<2, 32, false, TE><<<grid, Tl::THREADS, Tl::SMEM_BYTES, st>>>(
         mb, nmembers, nitems, parity);
+}
+
+cudaError_t launch_batch_step(int dtype, const void* members, int nmembers, int nitems, int grid,
+                              int parity, int packed, cudaStream_t st) {
+  const BatchMember* mb = reinterpret_cast<const BatchMember*>(members);
+  if (dtype == FSLBM_F32) launch_batch_t<float>(mb, nmembers, nitems, grid, parity, packed, st);
+  else if (dtype == FSLBM_F16) launch_batch_t<__half>(mb, nmembers, nitems, grid, parity, packed, st);
+  else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 
 cudaError_t launch_monitor(const MonitorLaunch& a, cudaStream_t st) {
   if (a.dtype == FSLBM_F32) monitor_kernel<float><<<1, 512, 0, st>>>(a);
   else if (a.dtype == FSLBM_F64) monitor_kernel<double><<<1, 512, 0, st>>>(a);
+  else if (a.dtype == FSLBM_F16) monitor_kernel<__half><<<1, 512, 0, st>>>(a);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -301,6 +354,8 @@ cudaError_t launch_zero_walls(int dtype, void* state, const uint8_t* mask, int l
     zero_walls_kernel<float><<<grid, 256, 0, st>>>(reinterpret_cast<float*>(state), mask, lxp, ly, L);
   else if (dtype == FSLBM_F64)
     zero_walls_kernel<double><<<grid, 256, 0, st>>>(reinterpret_cast<double*>(state), mask, lxp, ly, L);
+  else if (dtype == FSLBM_F16)
+    zero_walls_kernel<__half><<<grid, 256, 0, st>>>(reinterpret_cast<__half*>(state), mask, lxp, ly, L);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -333,6 +388,9 @@ cudaError_t launch_convert_in(int dtype, void* state, const void* src, int src_i
   } else if (dtype == FSLBM_F64) {
     if (src_is_f64) convert_in_kernel<double, double><<<grid, 256, 0, st>>>((double*)state, (const double*)src, lx, lxp, ly, L);
     else convert_in_kernel<double, float><<<grid, 256, 0, st>>>((double*)state, (const float*)src, lx, lxp, ly, L);
+  } else if (dtype == FSLBM_F16) {
+    if (src_is_f64) convert_in_kernel<__half, double><<<grid, 256, 0, st>>>((__half*)state, (const double*)src, lx, lxp, ly, L);
+    else convert_in_kernel<__half, float><<<grid, 256, 0, st>>>((__half*)state, (const float*)src, lx, lxp, ly, L);
   } else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -346,6 +404,9 @@ cudaError_t launch_convert_out(int dtype, const void* state, void* dst, int dst_
   } else if (dtype == FSLBM_F64) {
     if (dst_is_f64) convert_out_kernel<double, double><<<grid, 256, 0, st>>>((const double*)state, (double*)dst, lx, lxp, ly, L);
     else convert_out_kernel<double, float><<<grid, 256, 0, st>>>((const double*)state, (float*)dst, lx, lxp, ly, L);
+  } else if (dtype == FSLBM_F16) {
+    if (dst_is_f64) convert_out_kernel<__half, double><<<grid, 256, 0, st>>>((const __half*)state, (double*)dst, lx, lxp, ly, L);
+    else convert_out_kernel<__half, float><<<grid, 256, 0, st>>>((const __half*)state, (float*)dst, lx, lxp, ly, L);
   } else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -357,7 +418,7 @@ __global__ void check_kernel(const TS* s, size_t n, double* out) {
   double v[2] = {0, 0};
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < 4 * n;
        i += size_t(gridDim.x) * blockDim.x) {
-    const double a = double(s[i]);
+    const double a = to_d(s[i]);
     if (!isfinite(a)) v[0] += 1.0;
     else if (i >= n) v[1] = fmax(v[1], fabs(a));
   }
@@ -390,6 +451,7 @@ cudaError_t launch_check(int dtype, const void* state, size_t n_per_field, doubl
   if (e) return e;
   if (dtype == FSLBM_F32) check_kernel<float><<<296, 256, 0, st>>>((const float*)state, n_per_field, out);
   else if (dtype == FSLBM_F64) check_kernel<double><<<296, 256, 0, st>>>((const double*)state, n_per_field, out);
+  else if (dtype == FSLBM_F16) check_kernel<__half><<<296, 256, 0, st>>>((const __half*)state, n_per_field, out);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -405,20 +467,21 @@ __global__ void plane_stats_kernel(const TS* s, const uint8_t* mask, int lxp, in
                                    int d2, int xs, double pin_d, int cnt, double* acc) {
   const int Lr = L + 2 * d2;
   const size_t n = size_t(ly) * Lr, FS = size_t(lxp) * ly * L;
-  const TS pin = TS(pin_d);
+  using TA = typename ArithOf<TS>::type;
+  const TA pin = TA(pin_d);
   for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n;
        k += size_t(gridDim.x) * blockDim.x) {
     const int y = int(k % ly), zr = int(k / ly);
     int zc = zr - d2, jump = 0;
     if (zc < 0) { zc += L; jump = 1; } else if (zc >= L) { zc -= L; jump = -1; }
     const size_t o = (size_t(zc) * ly + y) * lxp + xs;
-    TS p = s[o];
+    TA p = TA(s[o]);
     if (mask[size_t(y) * lxp + xs] != kWall) {
-      if (jump == 1) p = TS(p + pin);
-      else if (jump == -1) p = TS(p - pin);
+      if (jump == 1) p = TA(p + pin);
+      else if (jump == -1) p = TA(p - pin);
     }
-    const double qp = double(p), qu = double(s[FS + o]), qv = double(s[2 * FS + o]),
-                 qw = double(s[3 * FS + o]);
+    const double qp = double(p), qu = to_d(s[FS + o]), qv = to_d(s[2 * FS + o]),
+                 qw = to_d(s[3 * FS + o]);
     const double c = double(cnt);
     double* a = acc;
     a[k] += qp;          const double dd1 = a[k] / c - qp;
@@ -443,6 +506,8 @@ cudaError_t launch_plane_stats(int dtype, const void* state, const uint8_t* mask
     plane_stats_kernel<float><<<grid, 256, 0, st>>>((const float*)state, mask, lxp, ly, L, d2, xs, pin, cnt, acc);
   else if (dtype == FSLBM_F64)
     plane_stats_kernel<double><<<grid, 256, 0, st>>>((const double*)state, mask, lxp, ly, L, d2, xs, pin, cnt, acc);
+  else if (dtype == FSLBM_F16)
+    plane_stats_kernel<__half><<<grid, 256, 0, st>>>((const __half*)state, mask, lxp, ly, L, d2, xs, pin, cnt, acc);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -461,7 +526,8 @@ __global__ void profile_kernel(const TS* s, int lxp, int ly, int L, double* acc)
   if (x < lxp) {
     for (int z = blockIdx.z * 8 + tz; z < L; z += gridDim.z * 8) {
       const size_t o = (size_t(z) * ly + y) * lxp + x;
-      const double p = s[o], u = s[FS + o], vv = s[2 * FS + o], w = s[3 * FS + o];
+      const double p = to_d(s[o]), u = to_d(s[FS + o]), vv = to_d(s[2 * FS + o]),
+                   w = to_d(s[3 * FS + o]);
       v[0] += p; v[1] += u; v[2] += vv; v[3] += w;
       v[4] += u * u; v[5] += vv * vv; v[6] += w * w; v[7] += u * vv; v[8] += u * w; v[9] += vv * w;
     }
@@ -485,6 +551,7 @@ cudaError_t launch_profile(int dtype, const void* state, int lxp, int ly, int L,
   if (grid.z < 1) grid.z = 1;
   if (dtype == FSLBM_F32) profile_kernel<float><<<grid, 256, 0, st>>>((const float*)state, lxp, ly, L, acc);
   else if (dtype == FSLBM_F64) profile_kernel<double><<<grid, 256, 0, st>>>((const double*)state, lxp, ly, L, acc);
+  else if (dtype == FSLBM_F16) profile_kernel<__half><<<grid, 256, 0, st>>>((const __half*)state, lxp, ly, L, acc);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -523,7 +590,7 @@ __global__ void gather_plane_kernel(const TS* s, int lx, int lxp, int ly, int L,
     size_t o;
     if (kind == 0) o = (r / ly * ly + r % ly) * lxp + idx;          // r = y + ly*z
     else o = (size_t(idx) * ly + r / lx) * lxp + r % lx;            // r = x + lx*y
-    out[k] = float(s[f * FS + o]);
+    out[k] = float(to_d(s[f * FS + o]));
   }
 }
 
@@ -533,6 +600,8 @@ cudaError_t launch_gather_plane(int dtype, const void* state, int lx, int lxp, i
     gather_plane_kernel<float><<<148, 256, 0, st>>>((const float*)state, lx, lxp, ly, L, kind, idx, out);
   else if (dtype == FSLBM_F64)
     gather_plane_kernel<double><<<148, 256, 0, st>>>((const double*)state, lx, lxp, ly, L, kind, idx, out);
+  else if (dtype == FSLBM_F16)
+    gather_plane_kernel<__half><<<148, 256, 0, st>>>((const __half*)state, lx, lxp, ly, L, kind, idx, out);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }

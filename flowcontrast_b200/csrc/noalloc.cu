@@ -87,7 +87,7 @@ int setup_device(int dev) {
   if (e != cudaSuccess)
     return fslbm_set_error(FSLBM_ERR_CUDA, "step_f32_noalloc: cudaGetSymbolAddress: %s",
                            cudaGetErrorString(e));
-  if ((e = step2_prepare(2, kNoallocTY)) != cudaSuccess)
+  if ((e = step2_prepare(FSLBM_F32, 2, kNoallocTY)) != cudaSuccess)
     return fslbm_set_error(FSLBM_ERR_CUDA, "step_f32_noalloc: kernel set-up: %s", cudaGetErrorString(e));
   int sms = 0;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
@@ -143,7 +143,7 @@ extern "C" int fslbm_step_f32_noalloc(const float* state_in, float* state_out,
 
   // tensor maps of the input state: p box (one-cell halo) and u,v,w box (corrector halo)
   int sw, ph, uh, hx, hy;
-  step2_box(2, kNoallocTY, &sw, &ph, &uh, &hx, &hy);
+  step2_box(FSLBM_F32, 2, kNoallocTY, &sw, &ph, &uh, &hx, &hy);
   const cuuint64_t fs = cuuint64_t(lx_pitch) * ly * lz;
   cuuint64_t dims[4] = {cuuint64_t(lx_pitch), cuuint64_t(ly), cuuint64_t(lz), 4};
   cuuint64_t strides[3] = {cuuint64_t(lx_pitch) * 4, cuuint64_t(lx_pitch) * ly * 4, fs * 4};

@@ -22,35 +22,41 @@
 #include <type_traits>
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <cuda_fp16.h>
 #include "common.h"
 #include "ptx.cuh"
 #include "step_kernel.cuh"
 
 namespace fslbm {
 
-template <int D1, int TY> struct Step2Tile {
+// TE is the storage type of the state (float, or __half for FP16 storage); arithmetic is FP32
+// either way. Halo widths and paddings keep every TMA box start and destination on 16 bytes.
+template <int D1, int TY, class TE = float> struct Step2Tile {
   static_assert(D1 % 2 == 0, "pair loads of the corrector taps need an even stride");
+  static constexpr int ES = int(sizeof(TE));
+  static constexpr int A16 = 16 / ES;                   // elements per 16 bytes
   static constexpr int TX = 32;
   static constexpr int THREADS = TX / 2 * TY;
   static constexpr int WARPS = THREADS / 32;
   static constexpr int R = 2 * D1;                      // farthest corrector tap
-  static constexpr int HX = (R + 3) / 4 * 4;            // x halo, TMA-aligned (16 bytes)
+  static constexpr int HX = (R + A16 - 1) / A16 * A16;  // x halo, TMA-aligned (16 bytes)
   static constexpr int HY = R;
   static constexpr int SW = TX + 2 * HX;                // row length of both boxes
   static constexpr int PH = TY + 2;                     // p rows (halo 1)
   static constexpr int UH = TY + 2 * HY;                // u,v,w rows
-  static constexpr int PPLANE = (SW * PH + 31) / 32 * 32;   // padded for 128-byte alignment
+  static constexpr int PPLANE = (SW * PH * ES + 127) / 128 * 128 / ES;   // 128-byte aligned
   static constexpr int UPLANE = SW * UH;
   static constexpr int SLOT = PPLANE + 3 * UPLANE;
   static constexpr int S = 8;                           // window slots (power of two)
   static constexpr int AHEAD = S - R - 1;               // planes loaded beyond the current one
   static_assert(AHEAD >= 1, "window too small for the corrector reach");
-  static constexpr uint32_t TX_BYTES = uint32_t((SW * PH + 3 * UPLANE) * 4);
-  static constexpr size_t RING_BYTES = size_t(S) * SLOT * 4;
+  static constexpr uint32_t TX_BYTES = uint32_t((SW * PH + 3 * UPLANE) * ES);
+  static constexpr size_t RING_BYTES = size_t(S) * SLOT * ES;
   static constexpr size_t BAR_OFFSET = RING_BYTES;
   static constexpr size_t SMEM_BYTES = BAR_OFFSET + 2 * S * sizeof(uint64_t);
-  static_assert((PPLANE * 4) % 128 == 0 && (UPLANE * 4) % 16 == 0 && (SLOT * 4) % 128 == 0,
+  static_assert((PPLANE * ES) % 128 == 0 && (UPLANE * ES) % 16 == 0 && (SLOT * ES) % 128 == 0,
                 "TMA destinations must stay aligned");
+  static_assert((HX * ES) % 16 == 0, "TMA box x start must be 16-byte aligned");
 };
 
 struct Step2Geom {
@@ -63,10 +69,56 @@ struct Step2Geom {
   const double* gauge;
   unsigned* err;
   long long* step_counter;
+  unsigned step_no;        // time step being computed (seed of the FP16 stochastic rounding)
 };
 
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 lds2(const float* p) { return *reinterpret_cast<const float2*>(p); }
+__device__ __forceinline__ float2 lds2(const __half* p) {
+  return __half22float2(*reinterpret_cast<const __half2*>(p));
+}
+
+// 32-bit integer hash (the "lowbias32" finaliser of C. Wellons' hash-prospector, public domain).
+__device__ __forceinline__ uint32_t hash32(uint32_t x) {
+  x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+  return x;
+}
+
+// FP32 -> FP16 with stochastic rounding: uniform noise below FP16's last kept mantissa bit
+// (the low 13 bits of an FP32 of FP16's normal range) is added to the magnitude, which is then
+// truncated. The result is unbiased, so increments far below half an FP16 ulp (the body force
+// and the slow relaxation of the step) survive in expectation instead of being rounded away.
+// In FP16's subnormal range the noise covers only part of the dropped bits (error < 2^-24).
+__device__ __forceinline__ __half sr_half(float x, uint32_t r) {
+  return __float2half_rz(__uint_as_float(__float_as_uint(x) + (r & 0x1fffu)));
+}
+
+// Stores of one column pair's four fields. FP32 storage stores the values; FP16 storage rounds
+// stochastically with noise from (pair index, field, time step) only, so a pipe's result does
+// not depend on which other work shares the launch.
+template <class TE> struct PairStore;
+template <> struct PairStore<float> {
+  static __device__ __forceinline__ void put(float* o, size_t fs, float2 p, float2 u, float2 v,
+                                             float2 w, const float*, uint32_t) {
+    *reinterpret_cast<float2*>(o) = p;
+    *reinterpret_cast<float2*>(o + fs) = u;
+    *reinterpret_cast<float2*>(o + 2 * fs) = v;
+    *reinterpret_cast<float2*>(o + 3 * fs) = w;
+  }
+};
+template <> struct PairStore<__half> {
+  static __device__ __forceinline__ __half2 sr2(float2 a, uint32_t r) {
+    return __halves2half2(sr_half(a.x, r), sr_half(a.y, r >> 16));
+  }
+  static __device__ __forceinline__ void put(__half* o, size_t fs, float2 p, float2 u, float2 v,
+                                             float2 w, const __half* base, uint32_t seed) {
+    const uint32_t key = uint32_t(o - base) << 2;
+    *reinterpret_cast<__half2*>(o) = sr2(p, hash32(key ^ seed));
+    *reinterpret_cast<__half2*>(o + fs) = sr2(u, hash32((key | 1u) ^ seed));
+    *reinterpret_cast<__half2*>(o + 2 * fs) = sr2(v, hash32((key | 2u) ^ seed));
+    *reinterpret_cast<__half2*>(o + 3 * fs) = sr2(w, hash32((key | 3u) ^ seed));
+  }
+};
 
 // Column-pair arithmetic: packed FP32x2 instructions (PK = true) or two scalar ones.
 template <bool PK> struct Pair;
@@ -120,17 +172,17 @@ __device__ __forceinline__ float2 qof(float2 P, float2 U, float2 V, float2 W) {
 // Marches one (tile, chunk) work item of one pipe: the step of every cell of the tile's columns
 // in the chunk's planes. `reinit` re-arms the CTA's mbarriers when the CTA has marched an item
 // before (persistent grids). Returns false when a bounded wait gave up (error flag set).
-template <int D1, int TY, bool PK>
+template <int D1, int TY, bool PK, class TE>
 __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUtensorMap* tmap_uvw,
                                             const Step2Geom& g, const StepConst<float>& k,
                                             int tile, int chunk, unsigned char* smem, bool reinit) {
-  using Tl = Step2Tile<D1, TY>;
+  using Tl = Step2Tile<D1, TY, TE>;
   using F = Pair<PK>;
   static_assert(D1 == 2, "the march prologue below is written for d1 = 2 (R = 4)");
   constexpr int R = Tl::R, HX = Tl::HX, HY = Tl::HY, SW = Tl::SW, S = Tl::S, AH = Tl::AHEAD;
   constexpr int PPL = Tl::PPLANE, UPL = Tl::UPLANE, SLOT = Tl::SLOT;
 
-  float* ring = reinterpret_cast<float*>(smem);
+  TE* ring = reinterpret_cast<TE*>(smem);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + Tl::BAR_OFFSET);
   uint64_t* empty = full + S;
 
@@ -170,7 +222,7 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
     const int slot = m & (S - 1);
     int zz = (start + dir * m) % g.L;
     if (zz < 0) zz += g.L;
-    float* dst = ring + slot * SLOT;
+    TE* dst = ring + slot * SLOT;
     mbar_arrive_expect_tx(&full[slot], Tl::TX_BYTES);
     tma_load_4d(dst, tmap_p, &full[slot], org.x - HX, org.y - 1, zz, 0);
     tma_load_4d(dst + PPL, tmap_uvw, &full[slot], org.x - HX, org.y - HY, zz, 1);
@@ -220,7 +272,9 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
 
   const float gauge = g.gauge ? float(*g.gauge) : 0.0f;
   const size_t FS = size_t(g.lxp) * g.ly * g.L;
-  float* outp = reinterpret_cast<float*>(g.out) + (size_t(start + dir * R) * g.ly + y) * g.lxp + xa;
+  const TE* obase = reinterpret_cast<const TE*>(g.out);
+  const uint32_t seed = hash32(g.step_no * 0x9e3779b9u + 0x632be5abu);
+  TE* outp = reinterpret_cast<TE*>(g.out) + (size_t(start + dir * R) * g.ly + y) * g.lxp + xa;
   const long long ostep = (long long)dir * g.ly * g.lxp;     // output pointer step per plane
   const int po = (ty + 1) * SW + HX + 2 * tp;                 // p box
   const int uo = PPL + (ty + HY) * SW + HX + 2 * tp;          // u box (v, w at +UPL, +2 UPL)
@@ -232,17 +286,23 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
   const float h6 = float(dir) / 72.0f;
 
   float2 hu[4], hv[4], hw[4];                                 // own columns of planes jo-4..jo-1
-  float aA[4][2], aB[4][2];                                   // predictor sums of the next outputs
+  // Predictor terms waiting for their output plane: b2 = the march-previous plane's share of the
+  // output being completed, b1 = the same for the next output, s1 = the self-plane moments of
+  // the next output. Each output sums its two neighbour planes' shares first (a commutative
+  // add) and then fuses its own plane's share, so the FP32 result of a cell does not depend on
+  // the march direction and hence not on how the pipe is split into streamwise chunks.
+  float b2[4][2], b1[4][2], s1[3][2];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     hu[j] = hv[j] = hw[j] = f2(0.f);
-    aA[j][0] = aA[j][1] = aB[j][0] = aB[j][1] = 0.f;
+    b2[j][0] = b2[j][1] = b1[j][0] = b1[j][1] = 0.f;
+    if (j < 3) s1[j][0] = s1[j][1] = 0.f;
   }
   float2 comp0, comp1, comp2, comp3;
 
   // predictor contribution of march plane ma (see step_kernel.cuh for the factorisation)
   auto predictor = [&](int ma) {
-    const float* ss = ring + (ma & (S - 1)) * SLOT;
+    const TE* ss = ring + (ma & (S - 1)) * SLOT;
     const int sp = start + dir * ma;                          // real plane
     const float off = sp < 0 ? k.pin : (sp >= g.L ? -k.pin : 0.0f);
     // Row-factored weights w(cx)w(cy) = {4,1,1}x{4,1,1}/36, per column of the pair: per row
@@ -252,8 +312,8 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
     float A[2][3], X[2][3], Y[2][3];
 #pragma unroll
     for (int cy = -1; cy <= 1; ++cy) {
-      const float* rp = ss + po + cy * SW;
-      const float* rq = ss + uo + cy * SW;
+      const TE* rp = ss + po + cy * SW;
+      const TE* rq = ss + uo + cy * SW;
       const float2 pL = lds2(rp - 2), pC = lds2(rp), pR = lds2(rp + 2);
       const float2 uL = lds2(rq - 2), uC = lds2(rq), uR = lds2(rq + 2);
       const float2 vL = lds2(rq + UPL - 2), vC = lds2(rq + UPL), vR = lds2(rq + UPL + 2);
@@ -304,8 +364,9 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
     }
     // True sums are A0'/36, dir A1'/12, A2'/8 (P1 and P2 were formed as P1/3 and P2/4.5).
     // Plane ma is the march-next neighbour of output ma-1 (completed here), itself, and the
-    // march-previous neighbour of ma+1: with e = (A0 + A2)/6 and h = A1/6,
-    // comp += e + h, aA = aB + (2/3) A0, aB = e - h (z-moment: comp += e + h, aB = h - e).
+    // march-previous neighbour of ma+1: with e = (A0 + A2)/6 and h = A1/6 the shares are
+    // e + h (next), (2/3) A0 (self) and e - h (previous); for the z-moment h - e (previous),
+    // none (self) and e + h (next), times dir.
     float cmp[4][2];
 #pragma unroll
     for (int col = 0; col < 2; ++col) {
@@ -319,18 +380,19 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
       const float eY = __fmaf_rn(Y[col][2], 1.0f / 48.0f, Y0 * (1.0f / 216.0f));
       const float hY = Y[col][1] * h6;
       const float sA = eA + hA;
-      cmp[0][col] = aA[0][col] + sA;
-      cmp[1][col] = aA[1][col] + (eX + hX);
-      cmp[2][col] = aA[2][col] + (eY + hY);
-      cmp[3][col] = aA[3][col] + sA;
-      aA[0][col] = __fmaf_rn(A0, 1.0f / 54.0f, aB[0][col]);
-      aA[1][col] = __fmaf_rn(X0, 1.0f / 54.0f, aB[1][col]);
-      aA[2][col] = __fmaf_rn(Y0, 1.0f / 54.0f, aB[2][col]);
-      aA[3][col] = aB[3][col];
-      aB[0][col] = eA - hA;
-      aB[1][col] = eX - hX;
-      aB[2][col] = eY - hY;
-      aB[3][col] = hA - eA;
+      cmp[0][col] = __fmaf_rn(s1[0][col], 1.0f / 54.0f, b2[0][col] + sA);
+      cmp[1][col] = __fmaf_rn(s1[1][col], 1.0f / 54.0f, b2[1][col] + (eX + hX));
+      cmp[2][col] = __fmaf_rn(s1[2][col], 1.0f / 54.0f, b2[2][col] + (eY + hY));
+      cmp[3][col] = b2[3][col] + sA;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) b2[q][col] = b1[q][col];
+      b1[0][col] = eA - hA;
+      b1[1][col] = eX - hX;
+      b1[2][col] = eY - hY;
+      b1[3][col] = hA - eA;
+      s1[0][col] = A0;
+      s1[1][col] = X0;
+      s1[2][col] = Y0;
     }
     comp0 = make_float2(cmp[0][0], cmp[0][1]);
     comp1 = make_float2(cmp[1][0], cmp[1][1]);
@@ -340,7 +402,7 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
 
   // own columns of march plane jo (for the history)
   auto own = [&](int jo, float2& uc, float2& vc, float2& wc) {
-    const float* so = ring + (jo & (S - 1)) * SLOT;
+    const TE* so = ring + (jo & (S - 1)) * SLOT;
     uc = lds2(so + uo); vc = lds2(so + uo + UPL); wc = lds2(so + uo + 2 * UPL);
   };
 
@@ -348,13 +410,13 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
   // overwritten with plane jo
   auto output = [&](int jo, auto rot_c) {
     constexpr int ROT = decltype(rot_c)::value;
-    const float* so = ring + (jo & (S - 1)) * SLOT;
-    const float* sa1 = ring + ((jo + D1) & (S - 1)) * SLOT;   // march planes ahead
-    const float* sa2 = ring + ((jo + 2 * D1) & (S - 1)) * SLOT;
+    const TE* so = ring + (jo & (S - 1)) * SLOT;
+    const TE* sa1 = ring + ((jo + D1) & (S - 1)) * SLOT;   // march planes ahead
+    const TE* sa2 = ring + ((jo + 2 * D1) & (S - 1)) * SLOT;
     const float2 pc = lds2(so + po);
     const float2 uc = lds2(so + uo), vc = lds2(so + uo + UPL), wc = lds2(so + uo + 2 * UPL);
     auto lap = [&](int f, float2 c, float2 zb1, float2 zb2) {
-      const float* q = so + uo + f * UPL;
+      const TE* q = so + uo + f * UPL;
       const float2 za1 = lds2(sa1 + uo + f * UPL), za2 = lds2(sa2 + uo + f * UPL);
       const float2 t1 = F::add(F::add(F::add(lds2(q - D1), lds2(q + D1)),
                                       F::add(lds2(q - D1 * SW), lds2(q + D1 * SW))),
@@ -377,10 +439,8 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
     const float2 vn = F::fma(F::add(F::fma(F::mul(dt, Lv), mm, vs), f2(k.fy)), tb, F::mul(vc, cc));
     const float2 wn = F::fma(F::add(F::fma(F::mul(dt, Lw), mm, wsz), f2(k.fz)), tb, F::mul(wc, cc));
     if (inside) {   // wall columns get zero (fl = 0)
-      *reinterpret_cast<float2*>(outp) = F::mul(rho, fl);
-      *reinterpret_cast<float2*>(outp + FS) = F::mul(un, fl);
-      *reinterpret_cast<float2*>(outp + 2 * FS) = F::mul(vn, fl);
-      *reinterpret_cast<float2*>(outp + 3 * FS) = F::mul(wn, fl);
+      PairStore<TE>::put(outp, FS, F::mul(rho, fl), F::mul(un, fl), F::mul(vn, fl),
+                         F::mul(wn, fl), obase, seed);
     }
     outp += ostep;
   };
@@ -432,14 +492,14 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
 }
 
 // One pipe, one step: CTA b marches (tile b % ntiles, chunk b / ntiles).
-template <int D1, int TY, bool PK>
-__global__ void __launch_bounds__(Step2Tile<D1, TY>::THREADS, 1)
+template <int D1, int TY, bool PK, class TE>
+__global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
     fslbm_step2_kernel(const __grid_constant__ CUtensorMap tmap_p,
                        const __grid_constant__ CUtensorMap tmap_uvw, const Step2Geom g,
                        const StepConst<float> k) {
   extern __shared__ __align__(128) unsigned char smem[];
   if (threadIdx.x == 0 && blockIdx.x == 0 && g.step_counter) *g.step_counter += 1;
-  step2_march<D1, TY, PK>(&tmap_p, &tmap_uvw, g, k, blockIdx.x % g.ntiles,
+  step2_march<D1, TY, PK, TE>(&tmap_p, &tmap_uvw, g, k, blockIdx.x % g.ntiles,
                           blockIdx.x / g.ntiles, smem, false);
 }
 
@@ -458,8 +518,8 @@ struct alignas(64) BatchMember {
 };
 
 // Many pipes, one step each: a persistent grid walks the work items of all members.
-template <int D1, int TY, bool PK>
-__global__ void __launch_bounds__(Step2Tile<D1, TY>::THREADS, 1)
+template <int D1, int TY, bool PK, class TE>
+__global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
     fslbm_step2_batch_kernel(const BatchMember* __restrict__ members, int nmembers, int nitems,
                              int parity) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -473,10 +533,11 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY>::THREADS, 1)
     g.out = mb.state[1 - cur];
     g.step_counter = nullptr;
     const long long done = *mb.steps;
+    g.step_no = unsigned(done + 1);
     g.gauge = (mb.monitor_every > 0 && done > 0 && done % mb.monitor_every == 0) ? mb.gauge_slot
                                                                               : nullptr;
     const int local = item - mb.item0;
-    if (!step2_march<D1, TY, PK>(&mb.map_p[cur], &mb.map_u[cur], g, mb.k, local % g.ntiles,
+    if (!step2_march<D1, TY, PK, TE>(&mb.map_p[cur], &mb.map_u[cur], g, mb.k, local % g.ntiles,
                                  local / g.ntiles, smem, !first))
       return;
     first = false;
