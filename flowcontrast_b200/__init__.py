@@ -13,7 +13,7 @@ import os
 
 import numpy as np
 
-__all__ = ["Context", "Solve", "Batch", "Domain", "Params", "FslbmError", "lib",
+__all__ = ["Context", "Solve", "Batch", "Server", "Domain", "Params", "FslbmError", "lib",
            "F64", "F32", "F16", "pipe_m_mask", "read_pipe_txt", "write_pipe_txt",
            "read_param_txt", "write_param_txt", "ref_mask_to_core", "init_poiseuille",
            "LIB_PATH"]
@@ -71,6 +71,48 @@ class Info(ctypes.Structure):
                 ("last_step_ms", ctypes.c_double), ("kernel_launches", ctypes.c_int64)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_int64), ("max_resident", ctypes.c_int),
+                ("quantum", ctypes.c_int)]
+
+
+class InitSpec(ctypes.Structure):
+    _fields_ = [("umax", ctypes.c_double), ("noise", ctypes.c_double), ("modes", ctypes.c_int),
+                ("mode_amp", ctypes.c_double), ("seed", ctypes.c_uint64)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("domain", Domain), ("params", Params), ("dtype", ctypes.c_int),
+                ("nsteps", ctypes.c_int64), ("init", ctypes.c_void_p * 4),
+                ("init_spec", InitSpec), ("out", ctypes.c_void_p * 4)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("error", ctypes.c_int),
+                ("steps_done", ctypes.c_int64), ("t_submit", ctypes.c_double),
+                ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double),
+                ("bytes_device", ctypes.c_int64), ("cells", ctypes.c_int64),
+                ("last", Monitor)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "last"}
+        d["last"] = self.last.as_dict()
+        return d
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64),
+                ("failed", ctypes.c_int64), ("queued", ctypes.c_int64),
+                ("resident", ctypes.c_int64), ("bytes_resident", ctypes.c_int64),
+                ("bytes_peak", ctypes.c_int64), ("rounds", ctypes.c_int64),
+                ("cell_steps", ctypes.c_double), ("busy_seconds", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
 _lib = None
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -120,6 +162,17 @@ def lib():
             "fslbm_batch_step": ([_vp, ctypes.c_int64, _i], _i),
             "fslbm_batch_sync": ([_vp], _i),
             "fslbm_batch_elapsed": ([_vp, ctypes.POINTER(ctypes.c_double)], _i),
+            "fslbm_solve_init_poiseuille": ([_vp, ctypes.c_double, ctypes.c_double, _i,
+                                             ctypes.c_double, ctypes.c_uint64], _i),
+            "fslbm_solve_footprint": ([ctypes.POINTER(Domain), _i, ctypes.POINTER(ctypes.c_int64)], _i),
+            "fslbm_server_create": ([_i, ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)], _i),
+            "fslbm_server_destroy": ([_vp], _i),
+            "fslbm_server_submit": ([_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)], _i),
+            "fslbm_server_poll": ([_vp, ctypes.c_int64, ctypes.POINTER(Result)], _i),
+            "fslbm_server_wait": ([_vp, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(Result)], _i),
+            "fslbm_server_drain": ([_vp, ctypes.c_double], _i),
+            "fslbm_server_release": ([_vp, ctypes.c_int64], _i),
+            "fslbm_server_stats_get": ([_vp, ctypes.POINTER(ServerStats)], _i),
             "fslbm_read_pipe_txt": ([ctypes.c_char_p, _i, _i, _i, _vp], _i),
             "fslbm_write_pipe_txt": ([ctypes.c_char_p, _i, _i, _i, _vp], _i),
             "fslbm_read_param_txt": ([ctypes.c_char_p, ctypes.POINTER(Params)], _i),
@@ -270,6 +323,11 @@ class Solve:
                 raise ValueError(f"field shape {a.shape} != {self.shape}")
         _check(lib().fslbm_solve_set_fields(self.handle, dt, *(_ptr(a) for a in arrs)))
 
+    def init_poiseuille(self, umax, noise=1e-3, modes=0, mode_amp=0.0, seed=1):
+        """The seeded start of init_poiseuille(), generated on the device."""
+        _check(lib().fslbm_solve_init_poiseuille(self.handle, float(umax), float(noise), int(modes),
+                                                 float(mode_amp), int(seed)))
+
     def set_fields_host(self, host_dtype, p, u, v, w):
         """Raw pointers (e.g. pinned host buffers) of the four fields."""
         _check(lib().fslbm_solve_set_fields(self.handle, host_dtype, p, u, v, w))
@@ -398,3 +456,81 @@ class Batch:
         if self.handle:
             _check(lib().fslbm_batch_destroy(self.handle))
             self.handle = None
+
+
+class Server:
+    """Served solves with continuous batching (fslbm_server_*): its own context and worker
+    thread on `device`. submit() returns a request id; results come back in FP32 arrays."""
+
+    def __init__(self, device=0, hbm_budget=0, max_resident=0, quantum=0):
+        cfg = ServerConfig(int(hbm_budget), int(max_resident), int(quantum))
+        h = ctypes.c_void_p()
+        _check(lib().fslbm_server_create(int(device), ctypes.byref(cfg), ctypes.byref(h)))
+        self.handle = h
+        self._out = {}
+
+    def submit(self, domain, params, dtype, nsteps, init=None, init_spec=None, want_fields=True):
+        """init: (4, lz, ly, lx) host fields (copied), or None with init_spec = dict(umax,
+        noise, modes, mode_amp, seed) for the device-generated start."""
+        r = Request()
+        r.domain = domain
+        r.params = params
+        r.dtype = int(dtype)
+        r.nsteps = int(nsteps)
+        keep = []
+        if init is not None:
+            a = np.ascontiguousarray(init, np.float32)
+            keep.append(a)
+            for k in range(4):
+                r.init[k] = a[k].ctypes.data
+        else:
+            q = dict(umax=0.1, noise=1e-3, modes=0, mode_amp=0.0, seed=1)
+            q.update(init_spec or {})
+            r.init_spec = InitSpec(q["umax"], q["noise"], int(q["modes"]), q["mode_amp"],
+                                   int(q["seed"]))
+        out = None
+        if want_fields:
+            out = np.empty((4, domain.lz, domain.ly, domain.lx), np.float32)
+            for k in range(4):
+                r.out[k] = out[k].ctypes.data
+        rid = ctypes.c_int64()
+        _check(lib().fslbm_server_submit(self.handle, ctypes.byref(r), ctypes.byref(rid)))
+        self._out[rid.value] = out
+        return rid.value
+
+    def poll(self, rid):
+        res = Result()
+        _check(lib().fslbm_server_poll(self.handle, int(rid), ctypes.byref(res)))
+        return res.as_dict()
+
+    def wait(self, rid, timeout=600.0):
+        res = Result()
+        _check(lib().fslbm_server_wait(self.handle, int(rid), float(timeout), ctypes.byref(res)))
+        return res.as_dict()
+
+    def fields(self, rid):
+        """Final fields (4, lz, ly, lx) FP32 of a finished request submitted with want_fields."""
+        return self._out.get(rid)
+
+    def drain(self, timeout=3600.0):
+        _check(lib().fslbm_server_drain(self.handle, float(timeout)))
+
+    def release(self, rid):
+        _check(lib().fslbm_server_release(self.handle, int(rid)))
+        return self._out.pop(rid, None)
+
+    def stats(self):
+        st = ServerStats()
+        _check(lib().fslbm_server_stats_get(self.handle, ctypes.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        if self.handle:
+            _check(lib().fslbm_server_destroy(self.handle))
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -118,6 +118,7 @@ struct fslbm_solve {
   fslbm_ctx* ctx = nullptr;
   int lx = 0, ly = 0, L = 0, lxp = 0, d2 = 10;
   double radius = 0, cx = 0, cy = 0;
+  bool from_mask = false;          // geometry given as a mask (else the analytic circle)
   int dtype = FSLBM_F32;
   size_t es = 4;
   fslbm_params prm{};
@@ -400,6 +401,7 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
     free_solve(s);
     return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: no fluid cells");
   }
+  s->from_mask = dom->mask != nullptr;
   s->radius = dom->radius > 0 ? dom->radius : std::sqrt(double(s->fluid2d) / M_PI);
   s->cx = dom->mask ? sxs / s->fluid2d : dom->cx;
   s->cy = dom->mask ? sys / s->fluid2d : dom->cy;
@@ -444,7 +446,9 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
   if ((e = dalloc(s, &s->d_scratch, 8 * sizeof(double)))) return fail("scratch");
   if ((e = cudaEventCreate(&s->ev0)) || (e = cudaEventCreate(&s->ev1))) return fail("events");
   if (int r = configure_kernel(s)) { free_solve(s); return r; }
-  if ((e = cudaDeviceSynchronize())) return fail("set-up");
+  // the set-up copies and memsets ran on the legacy stream; work already queued on other
+  // streams (other solves) is not waited for
+  if ((e = cudaStreamSynchronize(cudaStreamLegacy))) return fail("set-up");
   *out = s;
   return FSLBM_OK;
 }
@@ -511,6 +515,49 @@ extern "C" int fslbm_solve_set_fields(fslbm_solve* s, fslbm_dtype hd, const void
   // the other buffer's walls (never written by the step) must be zero too
   CUDA_TRY(launch_zero_walls(s->dtype, s->state[1 - s->cur], s->d_mask, s->lxp, s->ly, s->L, st));
   s->fields_set = true;
+  return FSLBM_OK;
+}
+
+int fslbm_poiseuille_setup(const fslbm_domain* dom, double umax, double noise, int modes,
+                           double mode_amp, uint64_t seed, fslbm::PoiseuilleInit* q,
+                           std::vector<uint8_t>* fluid_out);
+
+extern "C" int fslbm_solve_init_poiseuille(fslbm_solve* s, double umax, double noise, int modes,
+                                           double mode_amp, uint64_t seed) {
+  if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "init_poiseuille: null solve");
+  std::vector<uint8_t> dense;
+  fslbm_domain dom{};
+  dom.lx = s->lx; dom.ly = s->ly; dom.lz = s->L;
+  dom.radius = s->radius; dom.cx = s->cx; dom.cy = s->cy; dom.buffer_depth = s->d2;
+  if (s->from_mask) {
+    dense.resize(size_t(s->lx) * s->ly);
+    for (int y = 0; y < s->ly; ++y)
+      for (int x = 0; x < s->lx; ++x) dense[size_t(y) * s->lx + x] = s->mask[size_t(y) * s->lxp + x];
+    dom.mask = dense.data();
+  }
+  PoiseuilleInit q;
+  std::vector<uint8_t> fluid;
+  if (int r = fslbm_poiseuille_setup(&dom, umax, noise, modes, mode_amp, seed, &q, &fluid)) return r;
+  CUDA_TRY(cudaSetDevice(s->ctx->device));
+  cudaStream_t st = s->ctx->stream;
+  CUDA_TRY(launch_init_poiseuille(s->dtype, s->state[s->cur], s->d_mask, s->lxp, q, st));
+  CUDA_TRY(launch_zero_walls(s->dtype, s->state[1 - s->cur], s->d_mask, s->lxp, s->ly, s->L, st));
+  s->fields_set = true;
+  return FSLBM_OK;
+}
+
+// Device bytes fslbm_solve_create allocates for this domain and dtype (state ping-pong, mask,
+// column sums, tile list, monitor log and small buffers); a host-type read-back of a solve
+// whose storage type differs adds a staging buffer of 4 fields in that type.
+extern "C" int fslbm_solve_footprint(const fslbm_domain* dom, fslbm_dtype dtype, int64_t* bytes) {
+  if (!dom || !bytes || dom->lx < 1 || dom->ly < 1 || dom->lz < 1)
+    return fslbm_set_error(FSLBM_ERR_ARG, "solve_footprint: bad argument");
+  const int64_t es = dtype == FSLBM_F64 ? 8 : (dtype == FSLBM_F16 ? 2 : 4);
+  const int64_t lxp = (dom->lx + 7) / 8 * 8, cs = lxp * dom->ly, fs = cs * dom->lz;
+  const int64_t cc = dtype == FSLBM_F64 ? int64_t(sizeof(ColCoef<double>)) : int64_t(sizeof(ColCoef<float>));
+  const int64_t tiles = ((lxp + kTX - 1) / kTX) * ((dom->ly + kTY - 1) / kTY) * int64_t(sizeof(int2));
+  *bytes = 2 * 4 * fs * es + cs + cs * cc + tiles + int64_t(sizeof(DevCounters)) +
+           4096 * int64_t(sizeof(fslbm_monitor)) + int64_t(sizeof(double)) * 9 + int64_t(sizeof(unsigned));
   return FSLBM_OK;
 }
 

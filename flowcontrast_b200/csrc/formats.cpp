@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/fslbm.h"
+#include "noise.h"
 
 int fslbm_set_error(int code, const char* fmt, ...);
 
@@ -56,20 +57,6 @@ bool parse_int(const std::string& t, int* v) {
   if (!parse_double(t, &d) || d != std::floor(d) || std::fabs(d) > 2e9) return false;
   *v = int(d);
   return true;
-}
-
-uint64_t splitmix64(uint64_t x) {
-  // splitmix64 (Steele, Lea, Flood 2014): golden-ratio increment, two xor-shift-multiply rounds
-  uint64_t z = x + 0x9E3779B97F4A7C15ull;
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-  return z ^ (z >> 31);
-}
-
-// uniform in [-1, 1) from (seed, counter)
-double unit_pm(uint64_t seed, uint64_t counter) {
-  const uint64_t r = splitmix64(splitmix64(seed) ^ counter);
-  return double(r >> 11) * (2.0 / 9007199254740992.0) - 1.0;
 }
 
 }  // namespace
@@ -198,14 +185,18 @@ extern "C" int fslbm_ref_mask_to_core(const uint8_t* m, int lx, int ly, int lz_r
   return FSLBM_OK;
 }
 
-extern "C" int fslbm_init_poiseuille(const fslbm_domain* dom, double umax, double noise, int modes,
-                                     double mode_amp, uint64_t seed, double* p, double* u, double* v,
-                                     double* w) {
-  if (!dom || !p || !u || !v || !w || dom->lx < 1 || dom->ly < 1 || dom->lz < 1 || modes < 0)
-    return fslbm_set_error(FSLBM_ERR_ARG, "init_poiseuille: bad argument");
-  const int lx = dom->lx, ly = dom->ly, L = dom->lz;
+// Geometry of the seeded start (shared by the host and device generators): fluid cells from the
+// mask or the circle; for a mask (or no radius) the centre is the fluid centroid and R the
+// largest centre distance plus half a cell.
+int fslbm_poiseuille_setup(const fslbm_domain* dom, double umax, double noise, int modes,
+                           double mode_amp, uint64_t seed, fslbm::PoiseuilleInit* q,
+                           std::vector<uint8_t>* fluid_out) {
+  if (!dom || dom->lx < 1 || dom->ly < 1 || dom->lz < 1 || modes < 0 || modes > fslbm::kMaxInitModes)
+    return fslbm_set_error(FSLBM_ERR_ARG, "init_poiseuille: bad argument (modes <= %d)", fslbm::kMaxInitModes);
+  const int lx = dom->lx, ly = dom->ly;
   const size_t plane = size_t(lx) * ly;
-  std::vector<uint8_t> fluid(plane);
+  std::vector<uint8_t>& fluid = *fluid_out;
+  fluid.assign(plane, 0);
   double R = dom->radius, cx = dom->cx, cy = dom->cy;
   size_t nf = 0;
   double sx = 0, sy = 0;
@@ -228,32 +219,28 @@ extern "C" int fslbm_init_poiseuille(const fslbm_domain* dom, double umax, doubl
       }
     R = std::sqrt(r2max) + 0.5;
   }
-  // random phases of the perturbation modes
-  std::vector<double> ph(4 * size_t(modes));
-  for (int m = 0; m < modes; ++m)
-    for (int k = 0; k < 4; ++k) ph[4 * m + k] = M_PI * (1.0 + unit_pm(seed ^ 0xA5A5A5A5ull, 4ull * m + k));
-  for (int z = 0; z < L; ++z)
+  std::memset(q, 0, sizeof *q);
+  q->cx = cx; q->cy = cy; q->R = R; q->umax = umax; q->noise = noise; q->mode_amp = mode_amp;
+  q->seed = seed; q->lx = lx; q->ly = ly; q->L = dom->lz; q->modes = modes;
+  fslbm::poiseuille_phases(*q);
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_init_poiseuille(const fslbm_domain* dom, double umax, double noise, int modes,
+                                     double mode_amp, uint64_t seed, double* p, double* u, double* v,
+                                     double* w) {
+  if (!p || !u || !v || !w) return fslbm_set_error(FSLBM_ERR_ARG, "init_poiseuille: null output");
+  fslbm::PoiseuilleInit q;
+  std::vector<uint8_t> fluid;
+  if (int r = fslbm_poiseuille_setup(dom, umax, noise, modes, mode_amp, seed, &q, &fluid)) return r;
+  const size_t plane = size_t(q.lx) * q.ly;
+  for (int z = 0; z < q.L; ++z)
     for (size_t j = 0; j < plane; ++j) {
       const size_t idx = size_t(z) * plane + j;
       if (!fluid[j]) { p[idx] = u[idx] = v[idx] = w[idx] = 0.0; continue; }
-      const double dx = int(j % lx) - cx, dy = int(j / lx) - cy;
-      const double s2 = (dx * dx + dy * dy) / (R * R), s = std::sqrt(s2);
-      const double th = std::atan2(dy, dx);
-      double du = noise * umax * unit_pm(seed, 4 * idx + 1);
-      double dv = noise * umax * unit_pm(seed, 4 * idx + 2);
-      double dw = noise * umax * unit_pm(seed, 4 * idx + 3);
-      const double env = 2.6 * s * (1.0 - std::fmin(s2, 1.0));
-      for (int m = 0; m < modes; ++m) {
-        const double kz = 2.0 * M_PI * double(m + 1) * z / double(L);
-        const int n = 1 + m % 4;
-        dw += mode_amp * umax * env * std::sin(kz + ph[4 * m]) * std::cos(n * th + ph[4 * m + 1]);
-        du += mode_amp * umax * env * std::cos(kz + ph[4 * m + 2]) * std::sin(n * th + ph[4 * m + 3]);
-        dv += mode_amp * umax * env * std::sin(kz + ph[4 * m + 2]) * std::cos(n * th + ph[4 * m + 3]);
-      }
-      p[idx] = 0.0;
-      u[idx] = du;
-      v[idx] = dv;
-      w[idx] = -umax * std::fmax(0.0, 1.0 - s2) + dw;   // stored velocity is the negated physical one
+      double c[4];
+      fslbm::poiseuille_cell(q, int(j % q.lx), int(j / q.lx), z, c);
+      p[idx] = c[0]; u[idx] = c[1]; v[idx] = c[2]; w[idx] = c[3];
     }
   return FSLBM_OK;
 }

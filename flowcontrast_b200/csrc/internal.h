@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include "../../include/fslbm.h"
 #include "common.h"
+#include "noise.h"
 
 namespace fslbm {
 
@@ -86,6 +87,9 @@ cudaError_t launch_batch_step(int dtype, const void* members, int nmembers, int 
                               int packed, cudaStream_t st);
 cudaError_t launch_batch_monitor(const BatchMon* mons, int n, int parity_after, cudaStream_t st);
 
+// Seeded Poiseuille start written into a pitched state (walls and pad columns zero).
+cudaError_t launch_init_poiseuille(int dtype, void* state, const uint8_t* mask, int lxp,
+                                   const PoiseuilleInit& q, cudaStream_t st);
 cudaError_t launch_zero_walls(int dtype, void* state, const uint8_t* mask, int lxp, int ly, int L,
                               cudaStream_t st);
 cudaError_t launch_plane_stats(int dtype, const void* state, const uint8_t* mask, int lxp, int ly,

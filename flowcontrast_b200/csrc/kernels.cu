@@ -334,6 +334,36 @@ cudaError_t launch_monitor(const MonitorLaunch& a, cudaStream_t st) {
 }
 
 // ------------------------------------------------------------------------------------------
+// seeded initial fields generated on the device (same formula as the host generator)
+// ------------------------------------------------------------------------------------------
+template <class TS>
+__global__ void init_poiseuille_kernel(TS* s, const uint8_t* mask, int lxp, PoiseuilleInit q) {
+  const size_t FS = size_t(lxp) * q.ly * q.L;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < FS;
+       i += size_t(gridDim.x) * blockDim.x) {
+    const int x = int(i % lxp);
+    const size_t r = i / lxp;
+    const int y = int(r % q.ly), z = int(r / q.ly);
+    double c[4] = {0.0, 0.0, 0.0, 0.0};
+    if (x < q.lx && mask[size_t(y) * lxp + x] != kWall) poiseuille_cell(q, x, y, z, c);
+    s[i] = TS(c[0]); s[FS + i] = TS(c[1]); s[2 * FS + i] = TS(c[2]); s[3 * FS + i] = TS(c[3]);
+  }
+}
+
+cudaError_t launch_init_poiseuille(int dtype, void* state, const uint8_t* mask, int lxp,
+                                   const PoiseuilleInit& q, cudaStream_t st) {
+  const int grid = 1184;
+  if (dtype == FSLBM_F32)
+    init_poiseuille_kernel<float><<<grid, 256, 0, st>>>((float*)state, mask, lxp, q);
+  else if (dtype == FSLBM_F64)
+    init_poiseuille_kernel<double><<<grid, 256, 0, st>>>((double*)state, mask, lxp, q);
+  else if (dtype == FSLBM_F16)
+    init_poiseuille_kernel<__half><<<grid, 256, 0, st>>>((__half*)state, mask, lxp, q);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------
 // wall zeroing, conversion, check
 // ------------------------------------------------------------------------------------------
 template <class TS>

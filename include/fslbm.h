@@ -136,6 +136,12 @@ int fslbm_solve_kernel_time(fslbm_solve* s, double* ms_total, int64_t* launches)
 /* Device pointers of the current state (p, u, v, w in the solve's storage type, row pitch
  * info.lx_pitch). Valid until the next step, set_fields or destroy. */
 int fslbm_solve_device_fields(fslbm_solve* s, void** p, void** u, void** v, void** w);
+/* The seeded start of fslbm_init_poiseuille generated on the device into the solve's state
+ * (no host arrays, no copies); asynchronous on the context's stream. modes <= 16. */
+int fslbm_solve_init_poiseuille(fslbm_solve* s, double umax, double noise, int modes,
+                                double mode_amp, uint64_t seed);
+/* Device bytes fslbm_solve_create allocates for a domain and dtype (an upper bound). */
+int fslbm_solve_footprint(const fslbm_domain* dom, fslbm_dtype dtype, int64_t* bytes);
 
 /* ---- reference-layout fields: the core plus d2 buffer planes at each streamwise end,
  *      reconstructed as the bcond copies with the +-pin jump (FSLBM.cu:291-301) ---- */
@@ -177,6 +183,73 @@ int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int use_graph);
 int fslbm_batch_sync(fslbm_batch* b);
 /* Device time of the last fslbm_batch_step call (valid after fslbm_batch_sync). */
 int fslbm_batch_elapsed(fslbm_batch* b, double* ms);
+
+/* ---- served solves: a request loop with continuous batching (no reference counterpart) ----
+ * The server owns a context on `device` and a worker thread. Requests are admitted in arrival
+ * order while their device footprint fits the HBM budget (and the resident count its limit);
+ * their state stays on the device until they finish. Every round the worker advances all
+ * resident solves together, one batched launch per step per storage type, for
+ * min(quantum, fewest steps left) steps; requests that arrive meanwhile join at the next
+ * round, finished ones leave and free their memory. A solve's result does not depend on what
+ * else shares its rounds (the step is bitwise independent of the batch it runs in). */
+typedef struct {
+  int64_t hbm_budget;  /* bytes of solve state the server may hold; 0 = 150e9 */
+  int max_resident;    /* 0 = no limit */
+  int quantum;         /* steps per round; 0 = 50 */
+} fslbm_server_config;
+
+typedef struct {
+  double umax, noise;  /* see fslbm_init_poiseuille */
+  int modes;
+  double mode_amp;
+  uint64_t seed;
+} fslbm_init_spec;
+
+typedef struct {
+  fslbm_domain domain;     /* the mask, if any, is copied at submit */
+  fslbm_params params;
+  int dtype;               /* fslbm_dtype */
+  int64_t nsteps;
+  const float* init[4];    /* host FP32 initial p,u,v,w (lx*ly*lz, copied at submit), or all NULL */
+  fslbm_init_spec init_spec; /* the device-generated start used when init[0] is NULL */
+  float* out[4];           /* host FP32 buffers for the final fields, or all NULL; must stay
+                              valid until the request is done */
+} fslbm_request;
+
+enum { FSLBM_REQ_QUEUED = 0, FSLBM_REQ_RUNNING = 1, FSLBM_REQ_DONE = 2, FSLBM_REQ_FAILED = 3 };
+
+typedef struct {
+  int status;              /* FSLBM_REQ_* */
+  int error;               /* FSLBM_ERR_* of a failed request */
+  int64_t steps_done;
+  double t_submit, t_admit, t_done;  /* seconds since the server started (host clock) */
+  int64_t bytes_device;    /* footprint charged against the budget */
+  int64_t cells;           /* lx*ly*lz */
+  fslbm_monitor last;      /* latest monitor record (step 0 if none) */
+} fslbm_result;
+
+typedef struct {
+  int64_t submitted, completed, failed, queued, resident;
+  int64_t bytes_resident, bytes_peak;
+  int64_t rounds;
+  double cell_steps;       /* box cells x steps of the completed requests */
+  double busy_seconds;     /* wall time with at least one resident solve */
+} fslbm_server_stats;
+
+int fslbm_server_create(int device, const fslbm_server_config* cfg, fslbm_server** out);
+/* Stops the worker after the current round; unfinished requests are dropped. */
+int fslbm_server_destroy(fslbm_server* srv);
+/* Queues a request. FSLBM_ERR_BUDGET if it could never fit the budget, FSLBM_ERR_ARG for a
+ * domain or parameter set that fslbm_solve_create would reject. */
+int fslbm_server_submit(fslbm_server* srv, const fslbm_request* req, int64_t* id);
+int fslbm_server_poll(fslbm_server* srv, int64_t id, fslbm_result* out);
+/* Waits until the request is done or failed, at most timeout_s seconds (FSLBM_ERR_TIMEOUT). */
+int fslbm_server_wait(fslbm_server* srv, int64_t id, double timeout_s, fslbm_result* out);
+/* Waits until every submitted request is done or failed. */
+int fslbm_server_drain(fslbm_server* srv, double timeout_s);
+/* Forgets a finished request (its result can no longer be polled). */
+int fslbm_server_release(fslbm_server* srv, int64_t id);
+int fslbm_server_stats_get(fslbm_server* srv, fslbm_server_stats* out);
 
 /* ---- allocation-free step ---- */
 /* No counterpart in the reference. Advances a caller-owned FP32 state by one step (the same

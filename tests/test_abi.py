@@ -118,3 +118,29 @@ def test_ctx_create_without_gpu_reports_error(built):
     with pytest.raises(built.FslbmError) as e:
         built.Context(0)
     assert e.value.code == -2
+
+
+def test_server_without_gpu_reports_error(built):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    with pytest.raises(built.FslbmError) as e:
+        built.Server(0)
+    assert e.value.code == -2
+
+
+def test_solve_footprint_counts_state_ping_pong(built):
+    import ctypes
+    fb = built
+    dom = fb.make_domain(128, 128, 512, radius=63, cx=63.5, cy=63.5)
+    out = {}
+    for dt in (fb.F64, fb.F32, fb.F16):
+        b = ctypes.c_int64()
+        fb._check(fb.lib().fslbm_solve_footprint(ctypes.byref(dom), dt, ctypes.byref(b)))
+        out[dt] = b.value
+    state = 2 * 4 * 128 * 128 * 512
+    for dt, es in ((fb.F64, 8), (fb.F32, 4), (fb.F16, 2)):
+        assert state * es <= out[dt] <= state * es + 4 * 2 ** 20
