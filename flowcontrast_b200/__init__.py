@@ -162,6 +162,7 @@ def lib():
             "fslbm_batch_step": ([_vp, ctypes.c_int64, _i], _i),
             "fslbm_batch_sync": ([_vp], _i),
             "fslbm_batch_elapsed": ([_vp, ctypes.POINTER(ctypes.c_double)], _i),
+            "fslbm_batch_set_stop": ([_vp, _i, ctypes.c_int64], _i),
             "fslbm_solve_init_poiseuille": ([_vp, ctypes.c_double, ctypes.c_double, _i,
                                              ctypes.c_double, ctypes.c_uint64], _i),
             "fslbm_solve_footprint": ([ctypes.POINTER(Domain), _i, ctypes.POINTER(ctypes.c_int64)], _i),
@@ -446,6 +447,10 @@ class Batch:
 
     def sync(self):
         _check(lib().fslbm_batch_sync(self.handle))
+
+    def set_stop(self, member, stop_step):
+        """Member `member` stops stepping once its step count reaches stop_step (-1: never)."""
+        _check(lib().fslbm_batch_set_stop(self.handle, int(member), int(stop_step)))
 
     def elapsed_ms(self):
         ms = ctypes.c_double()

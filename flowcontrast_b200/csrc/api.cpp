@@ -2,6 +2,7 @@
 // ensemble and the device-side monitor log. The reference keeps all of this in main()
 // (FSLBM.cu:489-905); here it is a library with explicit error codes.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -978,12 +979,16 @@ extern "C" int fslbm_profile_reset(fslbm_solve* s) {
 struct fslbm_batch {
   fslbm_ctx* ctx = nullptr;
   std::vector<fslbm_solve*> members;
+  std::vector<int64_t> stop;       // per member: step count at which it stops (-1: never)
   bool fast = false;
   void* d_members = nullptr;
   BatchMon* d_mons = nullptr;
+  int2* d_items = nullptr;         // (member, item of the member), longest first
+  unsigned* d_tickets = nullptr;   // work-item counters, one per step parity
   std::vector<unsigned char> h_members;
   std::vector<BatchMon> h_mons;
-  int nitems = 0, grid = 0, packed = 1, chunk = 64;
+  std::vector<int2> h_items;
+  int nitems = 0, grid = 0, packed = 1, chunk = 32;
   cudaGraphExec_t exec2 = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
@@ -995,18 +1000,48 @@ static void free_batch(fslbm_batch* b) {
   if (b->exec2) cudaGraphExecDestroy(b->exec2);
   if (b->d_members) cudaFree(b->d_members);
   if (b->d_mons) cudaFree(b->d_mons);
+  if (b->d_items) cudaFree(b->d_items);
+  if (b->d_tickets) cudaFree(b->d_tickets);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   delete b;
 }
 
-// Member descriptors for the members' current buffers and step counts.
+// Work of one (tile, chunk) item of the column-pair kernel (TY = 32), for ordering the items:
+// planes marched (the chunk plus the 2R pipeline planes) times the tile's warps that compute
+// (two rows of 32 columns each) plus two for the pipeline's fixed cost.
+static int64_t item_cost(const fslbm_solve* s, int2 org, int nout) {
+  int warps = 0;
+  for (int w = 0; w < 16; ++w) {
+    bool any = false;
+    for (int r = 0; r < 2 && !any; ++r) {
+      const int y = org.y + 2 * w + r;
+      if (y >= s->ly) break;
+      for (int x = org.x; x < std::min(org.x + kTX, s->lxp) && !any; ++x)
+        any = s->mask[size_t(y) * s->lxp + x] == 0;
+    }
+    warps += any;
+  }
+  return int64_t(nout + 4 * s->prm.d1) * (warps + 2);
+}
+
+// Streamwise chunks of a member: about `chunk` planes each, at least 4*d1 planes.
+static int member_chunks(const fslbm_solve* s, int chunk) {
+  int nch = (s->L + chunk - 1) / chunk;
+  return std::max(1, std::min(nch, std::max(1, s->L / (4 * s->prm.d1))));
+}
+
+// Member descriptors for the members' current buffers, step counts and stops, and the work-item
+// table (rebuilt only when the membership or chunking changed: nitems == 0).
 static int batch_upload(fslbm_batch* b) {
   const size_t mbytes = batch_member_bytes();
   const int n = int(b->members.size());
+  cudaStream_t st = b->ctx->stream;
   b->h_members.assign(mbytes * n, 0);
   b->h_mons.resize(n);
-  int item = 0;
+  const bool build_items = b->h_items.empty();
+  struct Item { int64_t cost; int2 it; };
+  std::vector<Item> items;
   for (int i = 0; i < n; ++i) {
     fslbm_solve* s = b->members[i];
     StepLaunch a{};
@@ -1014,12 +1049,19 @@ static int batch_upload(fslbm_batch* b) {
     a.lxp = s->lxp; a.ly = s->ly; a.L = s->L; a.ntiles = s->ntiles;
     a.tiles = s->d_tiles; a.mask = s->d_mask; a.colcoef = s->d_colcoef; a.err = s->d_err;
     fill_constants(s, a);
-    int nch = (s->L + b->chunk - 1) / b->chunk;
-    nch = std::max(1, std::min(nch, std::max(1, s->L / (4 * s->prm.d1))));
+    const int nch = member_chunks(s, b->chunk);
+    const long long stop_at = b->stop[i] >= 0 ? (long long)b->stop[i] : LLONG_MAX;
     CUDA_TRY(fill_batch_member(b->h_members.data() + mbytes * i, s->maps2p, s->maps2u, a,
                                s->state[0], s->state[1], s->d_gauge, &s->d_counters->steps,
-                               s->prm.monitor_every, s->cur, nch, item));
-    item += s->ntiles * nch;
+                               stop_at, s->prm.monitor_every, s->cur, nch));
+    if (build_items) {
+      const std::vector<int2> tiles = fluid_tiles(s, s->ty2);
+      for (int c = 0; c < nch; ++c) {
+        const int nout = int((long long)s->L * (c + 1) / nch - (long long)s->L * c / nch);
+        for (int t = 0; t < int(tiles.size()); ++t)
+          items.push_back({item_cost(s, tiles[t], nout), make_int2(i, c * s->ntiles + t)});
+      }
+    }
     BatchMon& m = b->h_mons[i];
     std::memset(&m, 0, sizeof m);
     m.mon.dtype = s->dtype; m.mon.mask = s->d_mask;
@@ -1029,11 +1071,25 @@ static int batch_upload(fslbm_batch* b) {
     m.mon.log = s->d_log; m.mon.log_cap = s->log_cap; m.mon.gauge_out = s->d_gauge;
     m.mon.counters = s->d_counters;
     m.state[0] = s->state[0]; m.state[1] = s->state[1];
+    m.stop_at = stop_at;
     m.monitor_every = s->prm.monitor_every; m.cur0 = s->cur;
   }
-  b->nitems = item;
-  b->grid = std::max(1, std::min(item, b->ctx->sm_count));
-  cudaStream_t st = b->ctx->stream;
+  if (build_items) {
+    std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.cost > y.cost; });
+    b->h_items.resize(items.size());
+    for (size_t k = 0; k < items.size(); ++k) b->h_items[k] = items[k].it;
+    b->nitems = int(items.size());
+    b->grid = std::max(1, std::min(b->nitems, b->ctx->sm_count));
+    if (b->d_items) cudaFree(b->d_items);
+    b->d_items = nullptr;
+    CUDA_TRY(cudaMalloc(&b->d_items, std::max<size_t>(1, b->h_items.size()) * sizeof(int2)));
+    CUDA_TRY(cudaMemcpyAsync(b->d_items, b->h_items.data(), b->h_items.size() * sizeof(int2),
+                             cudaMemcpyHostToDevice, st));
+    if (b->exec2) {                // the graph holds the old table's address and size
+      cudaGraphExecDestroy(b->exec2);
+      b->exec2 = nullptr;
+    }
+  }
   CUDA_TRY(cudaMemcpyAsync(b->d_members, b->h_members.data(), b->h_members.size(),
                            cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaMemcpyAsync(b->d_mons, b->h_mons.data(), sizeof(BatchMon) * n,
@@ -1042,10 +1098,10 @@ static int batch_upload(fslbm_batch* b) {
 }
 
 static cudaError_t batch_enqueue_one(fslbm_batch* b, int parity, cudaStream_t st) {
-  cudaError_t e = launch_batch_step(b->members[0]->dtype, b->d_members, int(b->members.size()), b->nitems, b->grid,
-                                    parity, b->packed, st);
+  cudaError_t e = launch_batch_step(b->members[0]->dtype, b->d_members, b->d_items, b->nitems,
+                                    b->grid, parity, b->packed, b->d_tickets, st);
   if (e) return e;
-  return launch_batch_monitor(b->d_mons, int(b->members.size()), parity ^ 1, st);
+  return launch_batch_monitor(b->d_mons, int(b->members.size()), parity ^ 1, b->d_tickets, st);
 }
 
 extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, int n, fslbm_batch** out) {
@@ -1059,6 +1115,7 @@ extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, in
       return fslbm_set_error(FSLBM_ERR_ARG, "batch_create: member %d is null or of another context", i);
     }
     b->members.push_back(solves[i]);
+    b->stop.push_back(-1);
     fast = fast && solves[i]->use2 && solves[i]->ty2 == 32 && solves[i]->prm.d1 == 2 &&
            solves[i]->dtype == solves[0]->dtype;
   }
@@ -1069,6 +1126,8 @@ extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, in
   if (!e && fast) e = batch_prepare(solves[0]->dtype);
   if (!e && fast) e = cudaMalloc(&b->d_members, batch_member_bytes() * n);
   if (!e && fast) e = cudaMalloc(&b->d_mons, sizeof(BatchMon) * n);
+  if (!e && fast) e = cudaMalloc(&b->d_tickets, 2 * sizeof(unsigned));
+  if (!e && fast) e = cudaMemset(b->d_tickets, 0, 2 * sizeof(unsigned));
   if (!e) e = cudaEventCreate(&b->ev0);
   if (!e) e = cudaEventCreate(&b->ev1);
   if (e) {
@@ -1091,10 +1150,14 @@ extern "C" int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int use_graph) {
     if (!s->fields_set) return fslbm_set_error(FSLBM_ERR_STATE, "batch_step: a member has no fields");
   CUDA_TRY(cudaSetDevice(b->ctx->device));
   cudaStream_t st = b->ctx->stream;
+  // steps each member actually takes (a member stops at its stop step)
+  std::vector<int64_t> take(b->members.size(), nsteps);
+  for (size_t i = 0; i < b->members.size(); ++i)
+    if (b->stop[i] >= 0) take[i] = std::max<int64_t>(0, std::min(nsteps, b->stop[i] - b->members[i]->steps));
   if (!b->fast) {
     CUDA_TRY(cudaEventRecord(b->ev0, st));
-    for (fslbm_solve* s : b->members)
-      if (int r = enqueue_steps(s, nsteps)) return r;
+    for (size_t i = 0; i < b->members.size(); ++i)
+      if (int r = enqueue_steps(b->members[i], take[i])) return r;
     CUDA_TRY(cudaEventRecord(b->ev1, st));
     return FSLBM_OK;
   }
@@ -1120,11 +1183,19 @@ extern "C" int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int use_graph) {
   int parity = 0;
   for (; left > 0; --left, parity ^= 1) CUDA_TRY(batch_enqueue_one(b, parity, st));
   CUDA_TRY(cudaEventRecord(b->ev1, st));
-  for (fslbm_solve* s : b->members) {
-    s->steps += nsteps;
-    s->cur ^= int(nsteps & 1);
-    s->launches += 2 * nsteps;   // counted per member: each batched launch serves all members
+  for (size_t i = 0; i < b->members.size(); ++i) {
+    fslbm_solve* s = b->members[i];
+    s->steps += take[i];
+    s->cur ^= int(take[i] & 1);
+    s->launches += 2 * take[i];  // counted per member: each batched launch serves all members
   }
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_batch_set_stop(fslbm_batch* b, int member, int64_t stop_step) {
+  if (!b || member < 0 || member >= int(b->members.size()))
+    return fslbm_set_error(FSLBM_ERR_ARG, "batch_set_stop: bad batch or member index");
+  b->stop[member] = stop_step < 0 ? -1 : stop_step;
   return FSLBM_OK;
 }
 

@@ -73,6 +73,7 @@ cudaError_t launch_monitor(const MonitorLaunch& a, cudaStream_t st);
 struct BatchMon {
   MonitorLaunch mon;           // state is chosen per launch from `state`
   const void* state[2];
+  long long stop_at;           // no step (and no bookkeeping) once the counter reaches this
   int monitor_every;
   int cur0;
 };
@@ -81,11 +82,14 @@ size_t batch_member_bytes();
 // Writes one member descriptor (layout private to the kernels) into host memory at dst.
 cudaError_t fill_batch_member(void* dst, const CUtensorMap* map_p, const CUtensorMap* map_u,
                               const StepLaunch& a, void* state0, void* state1,
-                              const double* gauge_slot, const long long* steps, int monitor_every,
-                              int cur0, int nchunks, int item0);
-cudaError_t launch_batch_step(int dtype, const void* members, int nmembers, int nitems, int grid, int parity,
-                              int packed, cudaStream_t st);
-cudaError_t launch_batch_monitor(const BatchMon* mons, int n, int parity_after, cudaStream_t st);
+                              const double* gauge_slot, const long long* steps, long long stop_at,
+                              int monitor_every, int cur0, int nchunks);
+// items: nitems (member, item of the member) pairs; tickets: two counters (per step parity)
+// that start at zero; the bookkeeping launch resets the one its step used.
+cudaError_t launch_batch_step(int dtype, const void* members, const int2* items, int nitems,
+                              int grid, int parity, int packed, unsigned* tickets, cudaStream_t st);
+cudaError_t launch_batch_monitor(const BatchMon* mons, int n, int parity_after, unsigned* tickets,
+                                 cudaStream_t st);
 
 // Seeded Poiseuille start written into a pitched state (walls and pad columns zero).
 cudaError_t launch_init_poiseuille(int dtype, void* state, const uint8_t* mask, int lxp,

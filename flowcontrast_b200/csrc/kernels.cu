@@ -240,14 +240,19 @@ __global__ void monitor_kernel(MonitorLaunch a) {
 
 // Batched bookkeeping after a batched step: block i advances member i's step counter and, when
 // the member is due, writes its monitor record and the gauge of its next step.
-__global__ void batch_monitor_kernel(const BatchMon* mons, int parity_after) {
+__global__ void batch_monitor_kernel(const BatchMon* mons, int parity_after, unsigned* tickets) {
   __shared__ double sh[3 * 32];
   __shared__ int due;
   const BatchMon& b = mons[blockIdx.x];
   if (threadIdx.x == 0) {
-    const long long s = b.mon.counters->steps + 1;
-    b.mon.counters->steps = s;
-    due = b.monitor_every > 0 && s % b.monitor_every == 0;
+    if (blockIdx.x == 0) tickets[parity_after ^ 1] = 0u;   // the step that just ran is complete
+    const long long s0 = b.mon.counters->steps;
+    due = 0;
+    if (s0 < b.stop_at) {
+      const long long s = s0 + 1;
+      b.mon.counters->steps = s;
+      due = b.monitor_every > 0 && s % b.monitor_every == 0;
+    }
   }
   __syncthreads();
   if (!due) return;
@@ -257,8 +262,9 @@ __global__ void batch_monitor_kernel(const BatchMon* mons, int parity_after) {
   else monitor_body<float>(a, sh);
 }
 
-cudaError_t launch_batch_monitor(const BatchMon* mons, int n, int parity_after, cudaStream_t st) {
-  batch_monitor_kernel<<<n, 512, 0, st>>>(mons, parity_after);
+cudaError_t launch_batch_monitor(const BatchMon* mons, int n, int parity_after, unsigned* tickets,
+                                 cudaStream_t st) {
+  batch_monitor_kernel<<<n, 512, 0, st>>>(mons, parity_after, tickets);
   return cudaGetLastError();
 }
 
@@ -285,8 +291,8 @@ size_t batch_member_bytes() { return sizeof(BatchMember); }
 
 cudaError_t fill_batch_member(void* dst, const CUtensorMap* mp, const CUtensorMap* mu,
                               const StepLaunch& a, void* state0, void* state1,
-                              const double* gauge_slot, const long long* steps, int monitor_every,
-                              int cur0, int nchunks, int item0) {
+                              const double* gauge_slot, const long long* steps, long long stop_at,
+                              int monitor_every, int cur0, int nchunks) {
   BatchMember m;
   std::memset(&m, 0, sizeof m);
   m.map_p[0] = mp[0]; m.map_p[1] = mp[1];
@@ -298,29 +304,29 @@ cudaError_t fill_batch_member(void* dst, const CUtensorMap* mp, const CUtensorMa
   m.k.m = float(a.m); m.k.c0 = float(a.c0); m.k.c1 = float(a.c1); m.k.c2 = float(a.c2);
   m.k.fx = float(a.fx); m.k.fy = float(a.fy); m.k.fz = float(a.fz);
   m.state[0] = state0; m.state[1] = state1;
-  m.gauge_slot = gauge_slot; m.steps = steps; m.monitor_every = monitor_every;
-  m.cur0 = cur0; m.item0 = item0; m.nitems = a.ntiles * nchunks;
+  m.gauge_slot = gauge_slot; m.steps = steps; m.stop_at = stop_at;
+  m.monitor_every = monitor_every; m.cur0 = cur0;
   std::memcpy(dst, &m, sizeof m);
   return cudaSuccess;
 }
 
 template <class TE>
-static void launch_batch_t(const BatchMember* mb, int nmembers, int nitems, int grid, int parity,
-                           int packed, cudaStream_t st) {
+static void launch_batch_t(const BatchMember* mb, const int2* items, int nitems, int grid,
+                           int parity, int packed, unsigned* tickets, cudaStream_t st) {
   using Tl = Step2Tile<2, 32, TE>;
   if (packed)
     fslbm_step2_batch_kernel<2, 32, true, TE><<<grid, Tl::THREADS, Tl::SMEM_BYTES, st>>>(
-        mb, nmembers, nitems, parity);
+        mb, items, nitems, parity, tickets);
   else
     fslbm_step2_batch_kernel<2, 32, false, TE><<<grid, Tl::THREADS, Tl::SMEM_BYTES, st>>>(
-        mb, nmembers, nitems, parity);
+        mb, items, nitems, parity, tickets);
 }
 
-cudaError_t launch_batch_step(int dtype, const void* members, int nmembers, int nitems, int grid,
-                              int parity, int packed, cudaStream_t st) {
+cudaError_t launch_batch_step(int dtype, const void* members, const int2* items, int nitems,
+                              int grid, int parity, int packed, unsigned* tickets, cudaStream_t st) {
   const BatchMember* mb = reinterpret_cast<const BatchMember*>(members);
-  if (dtype == FSLBM_F32) launch_batch_t<float>(mb, nmembers, nitems, grid, parity, packed, st);
-  else if (dtype == FSLBM_F16) launch_batch_t<__half>(mb, nmembers, nitems, grid, parity, packed, st);
+  if (dtype == FSLBM_F32) launch_batch_t<float>(mb, items, nitems, grid, parity, packed, tickets, st);
+  else if (dtype == FSLBM_F16) launch_batch_t<__half>(mb, items, nitems, grid, parity, packed, tickets, st);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }

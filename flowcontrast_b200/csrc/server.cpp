@@ -3,11 +3,12 @@
 // no counterpart: it runs one pipe per process (FSLBM.cu:489-905).
 //
 // The worker owns its own context (one device, one stream) and uses only the public solve and
-// batch calls. A round is: launch min(quantum, fewest steps left) batched steps for every
-// storage type present; while those run, create and initialise the solves of requests that
-// fit the budget (their set-up is queued on the same stream, behind the round); wait for the
-// round; hand finished results back and free their memory. Client calls only touch the
-// request table under the mutex, so they are thread-safe and never wait for the GPU.
+// batch calls. A round is: launch min(quantum, most steps left) batched steps for every storage
+// type present, each member stopping at its own step budget (fslbm_batch_set_stop); while those
+// run, create and initialise the solves of requests that fit the budget (their set-up is
+// queued on the same stream, behind the round); wait for the round; hand finished results
+// back and free their memory. Client calls only touch the request table under the mutex, so
+// they are thread-safe and never wait for the GPU.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -43,6 +44,7 @@ using ReqPtr = std::shared_ptr<Request>;
 struct Group {
   int dtype = 0;
   std::vector<fslbm_solve*> members;
+  std::vector<int64_t> stops;     // each member's total step count
   fslbm_batch* batch = nullptr;
 };
 
@@ -64,7 +66,6 @@ struct fslbm_server {
   // worker-only
   std::vector<ReqPtr> active;
   std::vector<Group> groups;
-  int worker_error = 0;
 };
 
 namespace {
@@ -170,6 +171,7 @@ int regroup(fslbm_server* S) {
       it = next.end() - 1;
     }
     it->members.push_back(r->solve);
+    it->stops.push_back(r->req.nsteps);
   }
   for (Group& g : next) {
     auto old = std::find_if(S->groups.begin(), S->groups.end(), [&](const Group& o) {
@@ -178,9 +180,16 @@ int regroup(fslbm_server* S) {
     if (old != S->groups.end()) {
       g.batch = old->batch;
       old->batch = nullptr;
-    } else if (int rc = fslbm_batch_create(S->ctx, g.members.data(), int(g.members.size()), &g.batch)) {
-      for (Group& o : next) if (o.batch && &o != &g) fslbm_batch_destroy(o.batch);
-      return rc;
+    } else {
+      int rc = fslbm_batch_create(S->ctx, g.members.data(), int(g.members.size()), &g.batch);
+      for (int i = 0; !rc && i < int(g.members.size()); ++i)
+        rc = fslbm_batch_set_stop(g.batch, i, g.stops[i]);
+      if (rc) {
+        for (Group& o : next)
+          if (o.batch) fslbm_batch_destroy(o.batch);
+        for (Group& o : next) o.batch = nullptr;
+        return rc;
+      }
     }
   }
   for (Group& o : S->groups)
@@ -217,8 +226,9 @@ void run(fslbm_server* S) {
       fail_active(S, rc);
       continue;
     }
-    int64_t k = S->cfg.quantum;
-    for (const ReqPtr& r : S->active) k = std::min(k, r->left);
+    int64_t most = 0;
+    for (const ReqPtr& r : S->active) most = std::max(most, r->left);
+    const int64_t k = std::min<int64_t>(S->cfg.quantum, most);
     const auto tr = Clock::now();
     int rc = FSLBM_OK;
     for (Group& g : S->groups)
@@ -239,10 +249,11 @@ void run(fslbm_server* S) {
     }
     std::vector<ReqPtr> still;
     for (const ReqPtr& r : S->active) {
-      r->left -= k;
+      const int64_t took = std::min(k, r->left);
+      r->left -= took;
       {
         std::lock_guard<std::mutex> lk(S->mu);
-        r->res.steps_done += k;
+        r->res.steps_done += took;
       }
       if (r->left == 0) retire(S, r);
       else still.push_back(r);

@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
 }
 
 // One member of a batched ensemble: its tensor maps for both state buffers, its step geometry
-// and constants, and its share of the work items.
+// and constants, and where its step count stops.
 struct alignas(64) BatchMember {
   CUtensorMap map_p[2], map_u[2];
   Step2Geom g;                 // g.out is replaced by the buffer the step writes
@@ -512,33 +512,40 @@ struct alignas(64) BatchMember {
   void* state[2];
   const double* gauge_slot;    // the member's monitor p2, applied on the step after a monitor
   const long long* steps;      // the member's device step counter
+  long long stop_at;           // the member is not stepped once its counter reaches this
   int monitor_every;
   int cur0;                    // input buffer at batch parity 0
-  int item0, nitems;           // first work item and item count (tiles x chunks)
 };
 
-// Many pipes, one step each: a persistent grid walks the work items of all members.
+// Many pipes, one step each: a persistent grid claims work items from a ticket counter (one
+// per step parity; the bookkeeping launch after the step resets it). items[t] = (member, item
+// of that member), longest items first, so uneven members balance across the SMs.
 template <int D1, int TY, bool PK, class TE>
 __global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
-    fslbm_step2_batch_kernel(const BatchMember* __restrict__ members, int nmembers, int nitems,
-                             int parity) {
+    fslbm_step2_batch_kernel(const BatchMember* __restrict__ members, const int2* __restrict__ items,
+                             int nitems, int parity, unsigned* tickets) {
   extern __shared__ __align__(128) unsigned char smem[];
-  int mi = 0;
+  __shared__ int s_item;
   bool first = true;
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-    while (mi + 1 < nmembers && members[mi + 1].item0 <= item) ++mi;
-    const BatchMember& mb = members[mi];
+  for (;;) {
+    if (threadIdx.x == 0) s_item = int(atomicAdd(&tickets[parity], 1u));
+    __syncthreads();
+    const int t = s_item;
+    __syncthreads();               // every thread has read the ticket before the next claim
+    if (t >= nitems) return;
+    const int2 it = items[t];
+    const BatchMember& mb = members[it.x];
+    const long long done = *mb.steps;
+    if (done >= mb.stop_at) continue;
     const int cur = mb.cur0 ^ parity;
     Step2Geom g = mb.g;
     g.out = mb.state[1 - cur];
     g.step_counter = nullptr;
-    const long long done = *mb.steps;
     g.step_no = unsigned(done + 1);
     g.gauge = (mb.monitor_every > 0 && done > 0 && done % mb.monitor_every == 0) ? mb.gauge_slot
                                                                               : nullptr;
-    const int local = item - mb.item0;
-    if (!step2_march<D1, TY, PK, TE>(&mb.map_p[cur], &mb.map_u[cur], g, mb.k, local % g.ntiles,
-                                 local / g.ntiles, smem, !first))
+    if (!step2_march<D1, TY, PK, TE>(&mb.map_p[cur], &mb.map_u[cur], g, mb.k, it.y % g.ntiles,
+                                     it.y / g.ntiles, smem, !first))
       return;
     first = false;
   }

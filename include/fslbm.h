@@ -183,6 +183,10 @@ int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int use_graph);
 int fslbm_batch_sync(fslbm_batch* b);
 /* Device time of the last fslbm_batch_step call (valid after fslbm_batch_sync). */
 int fslbm_batch_elapsed(fslbm_batch* b, double* ms);
+/* Member `member` (index in the create call) is not stepped once its step count reaches
+ * stop_step (absolute; -1 = no stop), so members with different step budgets share launches;
+ * the others keep stepping. */
+int fslbm_batch_set_stop(fslbm_batch* b, int member, int64_t stop_step);
 
 /* ---- served solves: a request loop with continuous batching (no reference counterpart) ----
  * The server owns a context on `device` and a worker thread. Requests are admitted in arrival

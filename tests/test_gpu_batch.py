@@ -73,3 +73,31 @@ def test_batch_matches_members_alone(built, ctx, use_graph, dtype):
     b.close()
     for s in members:
         s.close()
+
+
+def test_batch_member_stops(built, ctx):
+    """Members with different step budgets share launches; each stops at its own budget and
+    equals the member stepped alone for that many steps."""
+    fb = built
+    specs = member_specs(n=4, seed=9)
+    budgets = [17, 40, 3, 33]
+    alone = []
+    for sp, n in zip(specs, budgets):
+        s = make_member(fb, ctx, sp)
+        s.step(n)
+        s.sync()
+        alone.append(s.get_fields(np.float32))
+        s.close()
+    members = [make_member(fb, ctx, sp) for sp in specs]
+    b = fb.Batch(ctx, members)
+    for i, n in enumerate(budgets):
+        b.set_stop(i, n)
+    b.step(25)
+    b.step(25)
+    b.sync()
+    for s, n, want in zip(members, budgets, alone):
+        assert s.info()["steps"] == n
+        assert np.array_equal(s.get_fields(np.float32), want)
+    b.close()
+    for s in members:
+        s.close()
