@@ -337,6 +337,249 @@ def run_ours(args, rank, world, local):
     return 0
 
 
+# ------------------------------------------------------------------------------------------
+# other workloads (one JSON line each; the default line above is the plain step)
+# ------------------------------------------------------------------------------------------
+def _member_start(fb, s, sp):
+    from flowcontrast_b200 import workloads as wl
+    s.init_poiseuille(2 * wl.U_BULK, noise=1e-3, modes=4, mode_amp=0.05, seed=sp.seed)
+
+
+def run_ensemble(args):
+    """Mixed-size ensemble (64 seeded pipes, L in [32,256], n in [24,96], Re in [50,3000],
+    FP32): the batched persistent launch against the same pipes stepped one at a time."""
+    import flowcontrast_b200 as fb
+    from flowcontrast_b200 import build, workloads as wl
+    build.build()
+    ctx = fb.Context(0)
+    specs = wl.ensemble(64, steps=args.steps)
+    cells = sum(sp.cells for sp in specs)
+
+    def fresh():
+        out = [fb.Solve(ctx, sp.domain(fb), sp.params(fb), fb.F32) for sp in specs]
+        for sp, s in zip(specs, out):
+            _member_start(fb, s, sp)
+        for s in out:
+            s.sync()
+        return out
+
+    # one at a time on the plain path (device time of each member's K steps, summed)
+    solves = fresh()
+    for s in solves:
+        s.step(args.warmup)
+    plain_ms = 0.0
+    for s in solves:
+        s.sync()
+        s.step(args.steps)
+        s.sync()
+        plain_ms += s.info()["last_step_ms"]
+    plain_fields = [s.get_fields(np.float32) for s in solves]
+    for s in solves:
+        s.close()
+
+    # batched: the same starts, one persistent launch per ensemble step, graph replay
+    solves = fresh()
+    b = fb.Batch(ctx, solves)
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    b.step(args.warmup)
+    b.sync()
+    t_w0 = time.time()
+    b.step(args.steps)
+    b.sync()
+    t_w1 = time.time()
+    batch_ms = b.elapsed_ms()
+    clocks = sampler.stop(t_w0, t_w1)
+    same = all(np.array_equal(s.get_fields(np.float32), want) for s, want in zip(solves, plain_fields))
+
+    # end to end: host starts in (pinned), K batched steps, fields out
+    import torch
+    host = [[torch.empty((sp.L, sp.n, sp.n), dtype=torch.float32).pin_memory() for _ in range(4)]
+            for sp in specs]
+    for f, h in zip(plain_fields, host):          # any host state of the right shape
+        for k in range(4):
+            h[k].copy_(torch.from_numpy(f[k]))
+    t0 = time.perf_counter()
+    for s, h in zip(solves, host):
+        s.set_fields_host(fb.F32, *[t.data_ptr() for t in h])
+    b.step(args.steps)
+    for s, h in zip(solves, host):
+        s.get_fields_host(fb.F32, *[t.data_ptr() for t in h])
+    for s in solves:
+        s.sync()
+    e2e_s = time.perf_counter() - t0
+    peak, peak_kind = hbm_peak()
+    value = cells * args.steps / (batch_ms * 1e-3) / 1e6
+    plain = cells * args.steps / (plain_ms * 1e-3) / 1e6
+    achieved = 32.0 * cells * args.steps / (batch_ms * 1e-3) / 1e9
+    line = {"metric": "aggregate MLUPS, batched ensemble (all box cells)", "value": value,
+            "unit": "MLUPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": batch_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ensemble)",
+            "config": {"workload": "64 seeded pipes, L~U[32,256] streamwise, n~U[24,96] square "
+                                   "cross-section, R=n/2-1, Re log-uniform [50,3000] (u_b 0.1), "
+                                   "tblend 0.02, d1 2, order-4 blend, FP32",
+                       "cells": cells, "members": len(specs),
+                       "l2": f"inputs larger than L2: {2 * 16 * cells / 1e9:.2f} GB of state"},
+            "plain_one_at_a_time_mlups": plain, "speedup_vs_plain": value / plain,
+            "batch_equals_plain_bitwise": bool(same),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": f"{peak_kind} hbm_gbs",
+                         "kernel": "fslbm_step2_batch_kernel<2,32,packed,float>"},
+            "e2e": {"value": cells * args.steps / e2e_s / 1e6, "unit": "MLUPS",
+                    "h2d_bytes_per_step": 16.0 * cells / args.steps,
+                    "d2h_bytes_per_step": 16.0 * cells / args.steps},
+            "gpu_launches": 2 * args.steps, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    b.close()
+    for s in solves:
+        s.close()
+    ctx.close()
+    return 0
+
+
+def _pct(xs, q):
+    return float(np.percentile(np.asarray(xs), q)) if xs else None
+
+
+def run_served(args):
+    """Served solves: a seeded Poisson stream (200 req/s) of pipe solves (32^3 .. 256x96x96
+    cells, 200..5000 steps, Re 50..5000, FP32 or FP16 storage) submitted in real time to the
+    continuous-batching server under a 150 GB budget."""
+    import flowcontrast_b200 as fb
+    from flowcontrast_b200 import build, workloads as wl
+    build.build()
+    reqs = wl.request_stream(args.requests, rate=200.0)
+    check = set(range(0, len(reqs), max(1, len(reqs) // 4)))     # requests checked afterwards
+    srv = fb.Server(0, hbm_budget=int(150e9), quantum=50)
+    # warm-up (kernel set-up and graph capture paths), not counted
+    for sp in reqs[:4]:
+        srv.submit(sp.domain(fb), sp.params(fb), sp.dtype, 20, want_fields=False,
+                   init_spec=dict(umax=0.2, seed=1))
+    srv.drain(600)
+    base = srv.stats()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    ids = []
+    t0 = time.perf_counter()
+    tw0 = time.time()
+    for k, sp in enumerate(reqs):
+        dt = t0 + sp.arrival - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        ids.append(srv.submit(sp.domain(fb), sp.params(fb), sp.dtype, sp.steps,
+                              want_fields=k in check,
+                              init_spec=dict(umax=2 * wl.U_BULK, noise=1e-3, modes=4,
+                                             mode_amp=0.05, seed=sp.seed)))
+    srv.drain(3600)
+    tw1 = time.time()
+    clocks = sampler.stop(tw0, tw1)
+    res = [srv.poll(i) for i in ids]
+    st = srv.stats()
+    lat = [r["t_done"] - r["t_submit"] for r in res if r["status"] == fb.REQ_DONE]
+    span = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
+    work = sum(r["cells"] * sp.steps for r, sp in zip(res, reqs) if r["status"] == fb.REQ_DONE)
+    # per-request checks: the same request alone (same dtype) must match bit for bit; the
+    # error against the FP64 solve of the same request is reported
+    ctx = fb.Context(0)
+    checks = []
+    for k in sorted(check):
+        sp, rid = reqs[k], ids[k]
+        got = srv.release(rid)
+        out = {}
+        for name, dt in (("same", sp.dtype), ("f64", fb.F64)):
+            s = fb.Solve(ctx, sp.domain(fb), sp.params(fb), dt)
+            s.init_poiseuille(2 * wl.U_BULK, noise=1e-3, modes=4, mode_amp=0.05, seed=sp.seed)
+            s.step(sp.steps)
+            s.sync()
+            out[name] = s.get_fields(np.float64)
+            s.close()
+        g = got.astype(np.float64)
+        checks.append({"request": k, "cells": sp.cells, "steps": sp.steps, "re": round(sp.re, 1),
+                       "dtype": "f16" if sp.dtype == fb.F16 else "f32",
+                       "equals_alone": bool(np.array_equal(g, out["same"])),
+                       "rel_l2_u_vs_f64": float(np.linalg.norm(g[1:] - out["f64"][1:]) /
+                                                np.linalg.norm(out["f64"][1:]))})
+    ctx.close()
+    srv.close()
+    line = {"metric": "aggregate MLUPS and p50/p95/p99 latency, served solves", "value": work / span / 1e6,
+            "unit": "MLUPS", "n_gpus": 1, "steps": len(reqs), "warmup": 4,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f16", "data": "synthetic (seeded Poisson request stream)",
+            "config": {"workload": f"{len(reqs)} requests, Poisson 200/s, cells log-uniform "
+                                   "32^3..256x96x96, steps U[200,5000], Re log-uniform [50,5000], "
+                                   "FP32 or FP16 storage 50/50, budget 150 GB, quantum 50",
+                       "requests": len(reqs)},
+            "latency_s": {"p50": _pct(lat, 50), "p95": _pct(lat, 95), "p99": _pct(lat, 99),
+                          "max": max(lat) if lat else None},
+            "completed": st["completed"] - base["completed"], "failed": st["failed"] - base["failed"],
+            "makespan_s": span, "busy_s": st["busy_seconds"] - base["busy_seconds"],
+            "rounds": st["rounds"] - base["rounds"], "peak_device_bytes": st["bytes_peak"],
+            "worker_seconds": {k: st[k] - base[k] for k in
+                               ("t_admit", "t_regroup", "t_launch", "t_wait", "t_retire")},
+            "checks": checks, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_mixed(args):
+    """Storage precision on the production pipe (512x128x128, Re 500/2000/5300): error of the
+    FP32 and FP16-storage forms against the FP64 solve after 200 steps, and their step rates."""
+    import flowcontrast_b200 as fb
+    from flowcontrast_b200 import build
+    build.build()
+    ctx = fb.Context(0)
+    dom = fb.make_domain(W["lx"], W["ly"], W["lz"], radius=W["R"], cx=W["cx"], cy=W["cy"])
+    cells = W["lx"] * W["ly"] * W["lz"]
+    out = {}
+    for re in (500.0, 2000.0, 5300.0):
+        ub = re * W["nu"] / (2 * W["R"])
+        g = (2 * (W["re_tau"] * W["nu"] / W["R"]) ** 2 / W["R"]) if re >= 5000 else 8 * W["nu"] * ub / W["R"] ** 2
+        prm = fb.Params.make(tblend=W["tblend"], pin=0.0, nu=W["nu"], d1=W["d1"], delta=1,
+                             blend=W["blend"], monitor_every=50, force=(0.0, 0.0, -g))
+        f = {}
+        for name, dt in (("f64", fb.F64), ("f32", fb.F32), ("f16", fb.F16)):
+            s = fb.Solve(ctx, dom, prm, dt)
+            s.init_poiseuille(2 * ub, noise=1e-3, modes=4, mode_amp=0.05, seed=W["seed"])
+            s.step(200)
+            s.sync()
+            f[name] = s.get_fields(np.float64)
+            s.close()
+        ref = f["f64"]
+        row = {}
+        for name in ("f32", "f16"):
+            row[name] = {"rel_l2_u": float(np.linalg.norm(f[name][1:] - ref[1:]) / np.linalg.norm(ref[1:])),
+                         "rel_l2_p": float(np.linalg.norm(f[name][0] - ref[0]) / np.linalg.norm(ref[0]))}
+        out[f"re{int(re)}"] = row
+    rates = {}
+    for name, dt in (("f64", fb.F64), ("f32", fb.F32), ("f16", fb.F16)):
+        s = fb.Solve(ctx, dom, fb.Params.make(tblend=W["tblend"], pin=0.0, nu=W["nu"], d1=W["d1"],
+                                              blend=W["blend"], monitor_every=50,
+                                              force=(0.0, 0.0, -physics()[2])), dt)
+        s.init_poiseuille(physics()[1], noise=1e-3, modes=4, mode_amp=0.05, seed=W["seed"])
+        s.step(args.warmup)
+        s.sync()
+        s.set_timing(True)
+        s.kernel_time()
+        s.step(args.steps)
+        s.sync()
+        ms, n = s.kernel_time()
+        rates[name] = cells / (ms / n * 1e-3) / 1e6
+        s.close()
+    ctx.close()
+    line = {"metric": "error vs FP64 after 200 steps and MLUPS per storage type", "value": rates["f16"],
+            "unit": "MLUPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": cells / rates["f16"] / 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f16 storage, f32 arithmetic", "data": "synthetic",
+            "config": {"workload": "512x128x128 pipe, R=63, tblend 0.02, d1 2, order 4, Re 500/2000/5300"},
+            "errors_200_steps": out, "mlups": rates, "f16_gain_vs_f32": rates["f16"] / rates["f32"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -345,11 +588,23 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--e2e-reps", type=int, default=3)
+    ap.add_argument("--workload", default="plain", choices=["plain", "ensemble", "served", "mixed"])
+    ap.add_argument("--requests", type=int, default=1000, help="served workload: request count")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     rank, world, local = dist_setup(args.gpus)
     try:
+        if args.workload != "plain":
+            if args.impl == "reference":
+                if rank == 0:
+                    print(json.dumps({"impl": "reference", "unavailable":
+                                      "the reference runs one pipe per process; it has no "
+                                      "batched, served or reduced-precision form"}), flush=True)
+                return 0
+            if world > 1:
+                raise SystemExit("--workload other than plain runs on one GPU")
+            return {"ensemble": run_ensemble, "served": run_served, "mixed": run_mixed}[args.workload](args)
         if args.impl == "reference":
             return run_reference_arm(args, rank, world, local)
         return run_ours(args, rank, world, local)

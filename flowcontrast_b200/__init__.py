@@ -105,7 +105,10 @@ class ServerStats(ctypes.Structure):
                 ("failed", ctypes.c_int64), ("queued", ctypes.c_int64),
                 ("resident", ctypes.c_int64), ("bytes_resident", ctypes.c_int64),
                 ("bytes_peak", ctypes.c_int64), ("rounds", ctypes.c_int64),
-                ("cell_steps", ctypes.c_double), ("busy_seconds", ctypes.c_double)]
+                ("cell_steps", ctypes.c_double), ("busy_seconds", ctypes.c_double),
+                ("t_admit", ctypes.c_double), ("t_regroup", ctypes.c_double),
+                ("t_launch", ctypes.c_double), ("t_wait", ctypes.c_double),
+                ("t_retire", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -52,11 +52,24 @@ extern "C" int fslbm_last_error(char* buf, size_t n) {
 // ------------------------------------------------------------------------------------------
 // context
 // ------------------------------------------------------------------------------------------
+// Device memory of a context's solves and batches comes from the context's own stream-ordered
+// pool, which keeps freed blocks (release threshold: never), so creating and destroying solves
+// in a serving loop neither maps nor unmaps device memory nor synchronises the device. All
+// set-up copies run on the context's stream, behind the allocations.
 struct fslbm_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaMemPool_t pool = nullptr;
   int sm_count = 0;
 };
+
+static cudaError_t ctx_alloc(fslbm_ctx* c, void** p, size_t bytes) {
+  return cudaMallocFromPoolAsync(p, std::max<size_t>(bytes, 1), c->pool, c->stream);
+}
+
+static void ctx_free(fslbm_ctx* c, void* p) {
+  if (p) cudaFreeAsync(p, c->stream);
+}
 
 extern "C" int fslbm_ctx_create(int device, fslbm_ctx** out) {
   if (!out) return fslbm_set_error(FSLBM_ERR_ARG, "ctx_create: null output");
@@ -74,9 +87,22 @@ extern "C" int fslbm_ctx_create(int device, fslbm_ctx** out) {
   c->device = device;
   c->sm_count = prop.multiProcessorCount;
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (!e) {
+    cudaMemPoolProps pp{};
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = device;
+    e = cudaMemPoolCreate(&c->pool, &pp);
+  }
+  if (!e) {
+    uint64_t keep = UINT64_MAX;
+    e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   if (e) {
+    if (c->pool) cudaMemPoolDestroy(c->pool);
+    if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
-    return fslbm_set_error(FSLBM_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    return fslbm_set_error(FSLBM_ERR_CUDA, "ctx_create: %s", cudaGetErrorString(e));
   }
   *out = c;
   return FSLBM_OK;
@@ -86,6 +112,7 @@ extern "C" int fslbm_ctx_destroy(fslbm_ctx* c) {
   if (!c) return FSLBM_OK;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  cudaMemPoolDestroy(c->pool);
   cudaStreamDestroy(c->stream);
   delete c;
   return FSLBM_OK;
@@ -137,6 +164,7 @@ struct fslbm_solve {
   // FP32 column-pair kernel (even d1): tile height, persistent grid, two maps per buffer
   bool use2 = false;
   int ty2 = 32, grid2 = 0, packed2 = 1;
+  std::vector<int> tile_warps;     // per column-pair tile: warps (two rows each) holding fluid
   CUtensorMap maps2p[2], maps2u[2];
   DevCounters* d_counters = nullptr;
   fslbm_monitor* d_log = nullptr;
@@ -257,15 +285,29 @@ static int configure_kernel(fslbm_solve* s) {
   const char* ep = std::getenv("FSLBM_PACKED");
   s->packed2 = (ep && std::atoi(ep) == 0) ? 0 : 1;
   const std::vector<int2> tiles = fluid_tiles(s, s->use2 ? s->ty2 : kTY);
+  s->tile_warps.clear();
+  if (s->use2)
+    for (const int2 org : tiles) {
+      int warps = 0;
+      for (int w = 0; w < s->ty2 / 2; ++w) {
+        bool any = false;
+        for (int y = org.y + 2 * w; y < std::min(org.y + 2 * w + 2, s->ly) && !any; ++y)
+          for (int x = org.x; x < std::min(org.x + kTX, s->lxp) && !any; ++x)
+            any = s->mask[size_t(y) * s->lxp + x] == 0;
+        warps += any;
+      }
+      s->tile_warps.push_back(warps);
+    }
   if (s->d_tiles) {
-    cudaFree(s->d_tiles);
+    ctx_free(s->ctx, s->d_tiles);
     s->bytes_device -= int64_t(s->ntiles) * sizeof(int2);
     s->d_tiles = nullptr;
   }
   s->ntiles = int(tiles.size());
-  CUDA_TRY(cudaMalloc(&s->d_tiles, tiles.size() * sizeof(int2)));
+  CUDA_TRY(ctx_alloc(s->ctx, reinterpret_cast<void**>(&s->d_tiles), tiles.size() * sizeof(int2)));
   s->bytes_device += int64_t(tiles.size() * sizeof(int2));
-  CUDA_TRY(cudaMemcpy(s->d_tiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpyAsync(s->d_tiles, tiles.data(), tiles.size() * sizeof(int2),
+                           cudaMemcpyHostToDevice, s->ctx->stream));
   if (s->use2) {
     CUDA_TRY(step2_prepare(s->dtype, s->prm.d1, s->ty2));
     // tiles x streamwise chunks, at most one CTA per SM slot and chunks of at least 2R planes
@@ -334,8 +376,7 @@ static void free_solve(fslbm_solve* s) {
   void* ptrs[] = {s->state[0], s->state[1], s->d_mask, s->d_colcoef, s->d_tiles, s->d_counters,
                   s->d_log, s->d_gauge, s->d_err, s->d_scratch, s->d_stats, s->d_prof,
                   s->d_stage, s->d_plane};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
+  for (void* p : ptrs) ctx_free(s->ctx, p);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
   for (cudaEvent_t e : s->tev) cudaEventDestroy(e);
@@ -344,7 +385,7 @@ static void free_solve(fslbm_solve* s) {
 
 template <class T>
 static cudaError_t dalloc(fslbm_solve* s, T** p, size_t bytes) {
-  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
+  cudaError_t e = ctx_alloc(s->ctx, reinterpret_cast<void**>(p), bytes);
   if (!e) s->bytes_device += int64_t(bytes);
   return e;
 }
@@ -422,34 +463,35 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
     free_solve(s);
     return r;
   };
+  // set-up on the context's stream (pageable host sources are staged before each call returns)
+  cudaStream_t st = ctx->stream;
   for (int b = 0; b < 2; ++b) {
     if ((e = dalloc(s, &s->state[b], 4 * fs * s->es))) return fail("state");
-    if ((e = cudaMemset(s->state[b], 0, 4 * fs * s->es))) return fail("memset");
+    if ((e = cudaMemsetAsync(s->state[b], 0, 4 * fs * s->es, st))) return fail("memset");
   }
   if ((e = dalloc(s, &s->d_mask, s->mask.size()))) return fail("mask");
-  cudaMemcpy(s->d_mask, s->mask.data(), s->mask.size(), cudaMemcpyHostToDevice);
+  if ((e = cudaMemcpyAsync(s->d_mask, s->mask.data(), s->mask.size(), cudaMemcpyHostToDevice, st)))
+    return fail("mask copy");
   if (dtype == FSLBM_F64) {
     auto cc = column_coefs<double>(s);
     if ((e = dalloc(s, &s->d_colcoef, cc.size() * sizeof(cc[0])))) return fail("colcoef");
-    cudaMemcpy(s->d_colcoef, cc.data(), cc.size() * sizeof(cc[0]), cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(s->d_colcoef, cc.data(), cc.size() * sizeof(cc[0]), cudaMemcpyHostToDevice, st);
   } else {
     auto cc = column_coefs<float>(s);
     if ((e = dalloc(s, &s->d_colcoef, cc.size() * sizeof(cc[0])))) return fail("colcoef");
-    cudaMemcpy(s->d_colcoef, cc.data(), cc.size() * sizeof(cc[0]), cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(s->d_colcoef, cc.data(), cc.size() * sizeof(cc[0]), cudaMemcpyHostToDevice, st);
   }
+  if (e) return fail("colcoef copy");
   if ((e = dalloc(s, &s->d_counters, sizeof(DevCounters)))) return fail("counters");
-  cudaMemset(s->d_counters, 0, sizeof(DevCounters));
+  if ((e = cudaMemsetAsync(s->d_counters, 0, sizeof(DevCounters), st))) return fail("memset");
   if ((e = dalloc(s, &s->d_log, sizeof(fslbm_monitor) * s->log_cap))) return fail("log");
   if ((e = dalloc(s, &s->d_gauge, sizeof(double)))) return fail("gauge");
-  cudaMemset(s->d_gauge, 0, sizeof(double));
+  if ((e = cudaMemsetAsync(s->d_gauge, 0, sizeof(double), st))) return fail("memset");
   if ((e = dalloc(s, &s->d_err, sizeof(unsigned)))) return fail("err");
-  cudaMemset(s->d_err, 0, sizeof(unsigned));
+  if ((e = cudaMemsetAsync(s->d_err, 0, sizeof(unsigned), st))) return fail("memset");
   if ((e = dalloc(s, &s->d_scratch, 8 * sizeof(double)))) return fail("scratch");
   if ((e = cudaEventCreate(&s->ev0)) || (e = cudaEventCreate(&s->ev1))) return fail("events");
   if (int r = configure_kernel(s)) { free_solve(s); return r; }
-  // the set-up copies and memsets ran on the legacy stream; work already queued on other
-  // streams (other solves) is not waited for
-  if ((e = cudaStreamSynchronize(cudaStreamLegacy))) return fail("set-up");
   *out = s;
   return FSLBM_OK;
 }
@@ -476,7 +518,7 @@ extern "C" int fslbm_solve_set_params(fslbm_solve* s, const fslbm_params* prm) {
 static int ensure_stage(fslbm_solve* s, size_t bytes) {
   if (s->stage_bytes >= bytes) return FSLBM_OK;
   if (s->d_stage) {
-    cudaFree(s->d_stage);
+    ctx_free(s->ctx, s->d_stage);
     s->bytes_device -= int64_t(s->stage_bytes);
     s->d_stage = nullptr;
     s->stage_bytes = 0;
@@ -690,7 +732,7 @@ extern "C" int fslbm_solve_sync(fslbm_solve* s) {
   unsigned err = 0;
   CUDA_TRY(cudaMemcpy(&err, s->d_err, sizeof err, cudaMemcpyDeviceToHost));
   if (err) {
-    cudaMemset(s->d_err, 0, sizeof(unsigned));
+    cudaMemsetAsync(s->d_err, 0, sizeof(unsigned), s->ctx->stream);
     return fslbm_set_error(FSLBM_ERR_TIMEOUT, "a bounded device wait gave up (flags 0x%x)", err);
   }
   return FSLBM_OK;
@@ -925,7 +967,8 @@ extern "C" int fslbm_stats_set(fslbm_solve* s, const double* means, int cnt, int
   std::vector<double> sums(11 * n);
   for (size_t k = 0; k < 4 * n; ++k) sums[k] = means[k] * double(cnt);        // FSLBM.cu:453-456
   for (size_t k = 4 * n; k < 11 * n; ++k) sums[k] = means[k] * double(cnt2);  // FSLBM.cu:457-463
-  CUDA_TRY(cudaMemcpy(s->d_stats, sums.data(), sums.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpyAsync(s->d_stats, sums.data(), sums.size() * sizeof(double),
+                           cudaMemcpyHostToDevice, s->ctx->stream));
   s->cnt = cnt; s->cnt2 = cnt2;
   return FSLBM_OK;
 }
@@ -984,11 +1027,13 @@ struct fslbm_batch {
   void* d_members = nullptr;
   BatchMon* d_mons = nullptr;
   int2* d_items = nullptr;         // (member, item of the member), longest first
-  unsigned* d_tickets = nullptr;   // work-item counters, one per step parity
+  unsigned* d_tickets = nullptr;   // [0..1] work-item counters per step parity, [2] error flag
   std::vector<unsigned char> h_members;
   std::vector<BatchMon> h_mons;
   std::vector<int2> h_items;
-  int nitems = 0, grid = 0, packed = 1, chunk = 32;
+  int nitems = 0, grid = 0, packed = 1;
+  int chunk = 64;                  // streamwise planes per work item (FSLBM_BATCH_CHUNK)
+  int chunk_used = 64;             // after shortening for small batches
   cudaGraphExec_t exec2 = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
@@ -998,31 +1043,20 @@ static void free_batch(fslbm_batch* b) {
   if (!b) return;
   cudaSetDevice(b->ctx->device);
   if (b->exec2) cudaGraphExecDestroy(b->exec2);
-  if (b->d_members) cudaFree(b->d_members);
-  if (b->d_mons) cudaFree(b->d_mons);
-  if (b->d_items) cudaFree(b->d_items);
-  if (b->d_tickets) cudaFree(b->d_tickets);
+  ctx_free(b->ctx, b->d_members);
+  ctx_free(b->ctx, b->d_mons);
+  ctx_free(b->ctx, b->d_items);
+  ctx_free(b->ctx, b->d_tickets);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   delete b;
 }
 
-// Work of one (tile, chunk) item of the column-pair kernel (TY = 32), for ordering the items:
-// planes marched (the chunk plus the 2R pipeline planes) times the tile's warps that compute
-// (two rows of 32 columns each) plus two for the pipeline's fixed cost.
-static int64_t item_cost(const fslbm_solve* s, int2 org, int nout) {
-  int warps = 0;
-  for (int w = 0; w < 16; ++w) {
-    bool any = false;
-    for (int r = 0; r < 2 && !any; ++r) {
-      const int y = org.y + 2 * w + r;
-      if (y >= s->ly) break;
-      for (int x = org.x; x < std::min(org.x + kTX, s->lxp) && !any; ++x)
-        any = s->mask[size_t(y) * s->lxp + x] == 0;
-    }
-    warps += any;
-  }
-  return int64_t(nout + 4 * s->prm.d1) * (warps + 2);
+// Work of one (tile, chunk) item of the column-pair kernel, for ordering the items: planes
+// marched (the chunk plus the 2R pipeline planes) times the tile's warps that compute plus two
+// for the pipeline's fixed cost.
+static int64_t item_cost(const fslbm_solve* s, int tile, int nout) {
+  return int64_t(nout + 4 * s->prm.d1) * (s->tile_warps[tile] + 2);
 }
 
 // Streamwise chunks of a member: about `chunk` planes each, at least 4*d1 planes.
@@ -1042,26 +1076,35 @@ static int batch_upload(fslbm_batch* b) {
   const bool build_items = b->h_items.empty();
   struct Item { int64_t cost; int2 it; };
   std::vector<Item> items;
+  if (build_items) {
+    // shorter chunks while there are fewer than two items per SM (few or small members)
+    auto count = [&](int chunk) {
+      int64_t c = 0;
+      for (fslbm_solve* s : b->members) c += int64_t(s->ntiles) * member_chunks(s, chunk);
+      return c;
+    };
+    b->chunk_used = b->chunk;
+    while (b->chunk_used > 8 && count(b->chunk_used) < 2 * b->ctx->sm_count) b->chunk_used /= 2;
+  }
   for (int i = 0; i < n; ++i) {
     fslbm_solve* s = b->members[i];
     StepLaunch a{};
     a.dtype = s->dtype; a.d1 = s->prm.d1;
     a.lxp = s->lxp; a.ly = s->ly; a.L = s->L; a.ntiles = s->ntiles;
-    a.tiles = s->d_tiles; a.mask = s->d_mask; a.colcoef = s->d_colcoef; a.err = s->d_err;
+    a.tiles = s->d_tiles; a.mask = s->d_mask; a.colcoef = s->d_colcoef;
+    a.err = b->d_tickets + 2;        // one flag for the whole batch
     fill_constants(s, a);
-    const int nch = member_chunks(s, b->chunk);
+    const int nch = member_chunks(s, b->chunk_used);
     const long long stop_at = b->stop[i] >= 0 ? (long long)b->stop[i] : LLONG_MAX;
     CUDA_TRY(fill_batch_member(b->h_members.data() + mbytes * i, s->maps2p, s->maps2u, a,
                                s->state[0], s->state[1], s->d_gauge, &s->d_counters->steps,
                                stop_at, s->prm.monitor_every, s->cur, nch));
-    if (build_items) {
-      const std::vector<int2> tiles = fluid_tiles(s, s->ty2);
+    if (build_items)
       for (int c = 0; c < nch; ++c) {
         const int nout = int((long long)s->L * (c + 1) / nch - (long long)s->L * c / nch);
-        for (int t = 0; t < int(tiles.size()); ++t)
-          items.push_back({item_cost(s, tiles[t], nout), make_int2(i, c * s->ntiles + t)});
+        for (int t = 0; t < s->ntiles; ++t)
+          items.push_back({item_cost(s, t, nout), make_int2(i, c * s->ntiles + t)});
       }
-    }
     BatchMon& m = b->h_mons[i];
     std::memset(&m, 0, sizeof m);
     m.mon.dtype = s->dtype; m.mon.mask = s->d_mask;
@@ -1080,9 +1123,9 @@ static int batch_upload(fslbm_batch* b) {
     for (size_t k = 0; k < items.size(); ++k) b->h_items[k] = items[k].it;
     b->nitems = int(items.size());
     b->grid = std::max(1, std::min(b->nitems, b->ctx->sm_count));
-    if (b->d_items) cudaFree(b->d_items);
+    ctx_free(b->ctx, b->d_items);
     b->d_items = nullptr;
-    CUDA_TRY(cudaMalloc(&b->d_items, std::max<size_t>(1, b->h_items.size()) * sizeof(int2)));
+    CUDA_TRY(ctx_alloc(b->ctx, reinterpret_cast<void**>(&b->d_items), b->h_items.size() * sizeof(int2)));
     CUDA_TRY(cudaMemcpyAsync(b->d_items, b->h_items.data(), b->h_items.size() * sizeof(int2),
                              cudaMemcpyHostToDevice, st));
     if (b->exec2) {                // the graph holds the old table's address and size
@@ -1124,10 +1167,10 @@ extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, in
   b->packed = solves[0]->packed2;
   cudaError_t e = cudaSetDevice(ctx->device);
   if (!e && fast) e = batch_prepare(solves[0]->dtype);
-  if (!e && fast) e = cudaMalloc(&b->d_members, batch_member_bytes() * n);
-  if (!e && fast) e = cudaMalloc(&b->d_mons, sizeof(BatchMon) * n);
-  if (!e && fast) e = cudaMalloc(&b->d_tickets, 2 * sizeof(unsigned));
-  if (!e && fast) e = cudaMemset(b->d_tickets, 0, 2 * sizeof(unsigned));
+  if (!e && fast) e = ctx_alloc(ctx, &b->d_members, batch_member_bytes() * n);
+  if (!e && fast) e = ctx_alloc(ctx, reinterpret_cast<void**>(&b->d_mons), sizeof(BatchMon) * n);
+  if (!e && fast) e = ctx_alloc(ctx, reinterpret_cast<void**>(&b->d_tickets), 4 * sizeof(unsigned));
+  if (!e && fast) e = cudaMemsetAsync(b->d_tickets, 0, 4 * sizeof(unsigned), ctx->stream);
   if (!e) e = cudaEventCreate(&b->ev0);
   if (!e) e = cudaEventCreate(&b->ev1);
   if (e) {
@@ -1204,11 +1247,15 @@ extern "C" int fslbm_batch_sync(fslbm_batch* b) {
   CUDA_TRY(cudaSetDevice(b->ctx->device));
   CUDA_TRY(cudaStreamSynchronize(b->ctx->stream));
   elapsed_if_recorded(b->ev0, b->ev1, &b->last_ms);
-  for (fslbm_solve* s : b->members) {
+  std::vector<unsigned*> flags;
+  if (b->fast) flags.push_back(b->d_tickets + 2);
+  else
+    for (fslbm_solve* s : b->members) flags.push_back(s->d_err);
+  for (unsigned* f : flags) {
     unsigned err = 0;
-    CUDA_TRY(cudaMemcpy(&err, s->d_err, sizeof err, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(&err, f, sizeof err, cudaMemcpyDeviceToHost));
     if (err) {
-      cudaMemset(s->d_err, 0, sizeof(unsigned));
+      cudaMemsetAsync(f, 0, sizeof(unsigned), b->ctx->stream);
       return fslbm_set_error(FSLBM_ERR_TIMEOUT, "batch_sync: a bounded device wait gave up");
     }
   }

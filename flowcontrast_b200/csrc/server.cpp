@@ -148,7 +148,17 @@ std::vector<ReqPtr> take_admissible(fslbm_server* S) {
   return out;
 }
 
-void admit(fslbm_server* S, const std::vector<ReqPtr>& adm) {
+// Creates the admitted requests' solves (their set-up is queued on the worker's stream) and
+// returns those with steps to take; requests of zero steps are retired at once.
+void add_time(fslbm_server* S, double fslbm_server_stats::*field, Clock::time_point t) {
+  const double d = std::chrono::duration<double>(Clock::now() - t).count();
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->st.*field += d;
+}
+
+std::vector<ReqPtr> admit(fslbm_server* S, const std::vector<ReqPtr>& adm) {
+  const auto t = Clock::now();
+  std::vector<ReqPtr> started;
   for (const ReqPtr& r : adm) {
     const int rc = start_request(S, r);
     if (rc) {
@@ -156,8 +166,10 @@ void admit(fslbm_server* S, const std::vector<ReqPtr>& adm) {
       continue;
     }
     if (r->left == 0) retire(S, r);
-    else S->active.push_back(r);
+    else started.push_back(r);
   }
+  add_time(S, &fslbm_server_stats::t_admit, t);
+  return started;
 }
 
 // Rebuilds the per-dtype groups whose membership changed.
@@ -219,11 +231,14 @@ void run(fslbm_server* S) {
       if (S->stop) break;
     }
     if (S->active.empty()) {
-      admit(S, take_admissible(S));
+      S->active = admit(S, take_admissible(S));
       continue;
     }
-    if (int rc = regroup(S)) {
-      fail_active(S, rc);
+    const auto tg = Clock::now();
+    const int rg = regroup(S);
+    add_time(S, &fslbm_server_stats::t_regroup, tg);
+    if (rg) {
+      fail_active(S, rg);
       continue;
     }
     int64_t most = 0;
@@ -233,10 +248,13 @@ void run(fslbm_server* S) {
     int rc = FSLBM_OK;
     for (Group& g : S->groups)
       if (!rc) rc = fslbm_batch_step(g.batch, k, 1);
+    add_time(S, &fslbm_server_stats::t_launch, tr);
     // set-up of new arrivals overlaps the round; they join the next one
-    std::vector<ReqPtr> adm = rc ? std::vector<ReqPtr>{} : take_admissible(S);
+    std::vector<ReqPtr> started = rc ? std::vector<ReqPtr>{} : admit(S, take_admissible(S));
+    const auto tw = Clock::now();
     for (Group& g : S->groups)
       if (!rc) rc = fslbm_batch_sync(g.batch);
+    add_time(S, &fslbm_server_stats::t_wait, tw);
     {
       std::lock_guard<std::mutex> lk(S->mu);
       S->st.busy_seconds += std::chrono::duration<double>(Clock::now() - tr).count();
@@ -244,10 +262,11 @@ void run(fslbm_server* S) {
     }
     if (rc) {
       fail_active(S, rc);
-      admit(S, adm);
+      S->active = started;
       continue;
     }
     std::vector<ReqPtr> still;
+    const auto tt = Clock::now();
     for (const ReqPtr& r : S->active) {
       const int64_t took = std::min(k, r->left);
       r->left -= took;
@@ -258,8 +277,9 @@ void run(fslbm_server* S) {
       if (r->left == 0) retire(S, r);
       else still.push_back(r);
     }
+    add_time(S, &fslbm_server_stats::t_retire, tt);
+    still.insert(still.end(), started.begin(), started.end());
     S->active.swap(still);
-    admit(S, adm);
   }
   fail_active(S, FSLBM_ERR_STATE);
   for (Group& g : S->groups)

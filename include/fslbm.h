@@ -237,7 +237,10 @@ typedef struct {
   int64_t bytes_resident, bytes_peak;
   int64_t rounds;
   double cell_steps;       /* box cells x steps of the completed requests */
-  double busy_seconds;     /* wall time with at least one resident solve */
+  double busy_seconds;     /* wall time from each round's launch to its completion */
+  /* worker time by activity (seconds): creating admitted solves, rebuilding the batches,
+   * launching rounds, waiting for rounds, handing back finished requests */
+  double t_admit, t_regroup, t_launch, t_wait, t_retire;
 } fslbm_server_stats;
 
 int fslbm_server_create(int device, const fslbm_server_config* cfg, fslbm_server** out);
