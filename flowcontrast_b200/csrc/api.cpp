@@ -164,7 +164,7 @@ struct fslbm_solve {
   // FP32 column-pair kernel (even d1): tile height, persistent grid, two maps per buffer
   bool use2 = false;
   int ty2 = 32, grid2 = 0, packed2 = 1;
-  std::vector<int> tile_warps;     // per column-pair tile: warps (two rows each) holding fluid
+  std::vector<int> tile_warps;     // per column-pair tile: batched-kernel warps (16 x 4 cells) holding fluid
   CUtensorMap maps2p[2], maps2u[2];
   DevCounters* d_counters = nullptr;
   fslbm_monitor* d_log = nullptr;
@@ -289,10 +289,11 @@ static int configure_kernel(fslbm_solve* s) {
   if (s->use2)
     for (const int2 org : tiles) {
       int warps = 0;
-      for (int w = 0; w < s->ty2 / 2; ++w) {
+      for (int w = 0; w < s->ty2 / 2; ++w) {       // warp w: columns 16*(w%2).., rows 4*(w/2)..
+        const int x0 = org.x + 16 * (w & 1), y0 = org.y + 4 * (w >> 1);
         bool any = false;
-        for (int y = org.y + 2 * w; y < std::min(org.y + 2 * w + 2, s->ly) && !any; ++y)
-          for (int x = org.x; x < std::min(org.x + kTX, s->lxp) && !any; ++x)
+        for (int y = y0; y < std::min(y0 + 4, s->ly) && !any; ++y)
+          for (int x = x0; x < std::min(x0 + 16, s->lxp) && !any; ++x)
             any = s->mask[size_t(y) * s->lxp + x] == 0;
         warps += any;
       }
@@ -1164,7 +1165,10 @@ extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, in
   }
   b->fast = fast;
   if (const char* ec = std::getenv("FSLBM_BATCH_CHUNK")) b->chunk = std::max(8, std::atoi(ec));
-  b->packed = solves[0]->packed2;
+  // packed FP32x2 pair arithmetic (measured 2 % faster than scalar pairs in the batched kernel
+  // despite a small register spill); FSLBM_BATCH_PACKED=0 selects scalar pairs
+  const char* ebp = std::getenv("FSLBM_BATCH_PACKED");
+  b->packed = (ebp && std::atoi(ebp) == 0) ? 0 : 1;
   cudaError_t e = cudaSetDevice(ctx->device);
   if (!e && fast) e = batch_prepare(solves[0]->dtype);
   if (!e && fast) e = ctx_alloc(ctx, &b->d_members, batch_member_bytes() * n);
