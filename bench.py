@@ -377,9 +377,28 @@ def run_ensemble(args):
     for s in solves:
         s.close()
 
-    # batched: the same starts, one persistent launch per ensemble step, graph replay
+    # batched, default tiling (the shipped table): the same starts, one persistent launch per
+    # ensemble step, graph replay
     solves = fresh()
     b = fb.Batch(ctx, solves)
+    b.step(args.warmup)
+    b.sync()
+    b.step(args.steps)
+    b.sync()
+    default_ms = b.elapsed_ms()
+    same = all(np.array_equal(s.get_fields(np.float32), want) for s, want in zip(solves, plain_fields))
+    b.close()
+    for s in solves:
+        s.close()
+
+    # batched after the autotuner (tiling per size class timed on this batch, state restored)
+    import tempfile
+    solves = fresh()
+    b = fb.Batch(ctx, solves)
+    t_tune = time.perf_counter()
+    tune_path = args.tuning_out or os.path.join(tempfile.mkdtemp(), "batch_tiling.json")
+    table = b.autotune(trial_steps=20, path=tune_path)
+    t_tune = time.perf_counter() - t_tune
     sampler = ClockSampler(0)
     sampler.start()
     time.sleep(0.3)
@@ -391,7 +410,8 @@ def run_ensemble(args):
     t_w1 = time.time()
     batch_ms = b.elapsed_ms()
     clocks = sampler.stop(t_w0, t_w1)
-    same = all(np.array_equal(s.get_fields(np.float32), want) for s, want in zip(solves, plain_fields))
+    same = same and all(np.array_equal(s.get_fields(np.float32), want)
+                        for s, want in zip(solves, plain_fields))
 
     # end to end: host starts in (pinned), K batched steps, fields out
     import torch
@@ -423,6 +443,8 @@ def run_ensemble(args):
                        "cells": cells, "members": len(specs),
                        "l2": f"inputs larger than L2: {2 * 16 * cells / 1e9:.2f} GB of state"},
             "plain_one_at_a_time_mlups": plain, "speedup_vs_plain": value / plain,
+            "default_tiling_mlups": cells * args.steps / (default_ms * 1e-3) / 1e6,
+            "autotune": {"seconds": t_tune, "classes": len(table), "trial_steps": 20},
             "batch_equals_plain_bitwise": bool(same),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
@@ -590,6 +612,7 @@ def main():
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--workload", default="plain", choices=["plain", "ensemble", "served", "mixed"])
     ap.add_argument("--requests", type=int, default=1000, help="served workload: request count")
+    ap.add_argument("--tuning-out", default=None, help="ensemble workload: write the tuned tiling table here")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

@@ -166,6 +166,9 @@ def lib():
             "fslbm_batch_sync": ([_vp], _i),
             "fslbm_batch_elapsed": ([_vp, ctypes.POINTER(ctypes.c_double)], _i),
             "fslbm_batch_set_stop": ([_vp, _i, ctypes.c_int64], _i),
+            "fslbm_batch_set_tiling": ([_vp, _i, _i, _i], _i),
+            "fslbm_batch_load_tiling": ([_vp, ctypes.c_char_p], _i),
+            "fslbm_batch_autotune": ([_vp, _i, ctypes.c_char_p], _i),
             "fslbm_solve_init_poiseuille": ([_vp, ctypes.c_double, ctypes.c_double, _i,
                                              ctypes.c_double, ctypes.c_uint64], _i),
             "fslbm_solve_footprint": ([ctypes.POINTER(Domain), _i, ctypes.POINTER(ctypes.c_int64)], _i),
@@ -454,6 +457,23 @@ class Batch:
     def set_stop(self, member, stop_step):
         """Member `member` stops stepping once its step count reaches stop_step (-1: never)."""
         _check(lib().fslbm_batch_set_stop(self.handle, int(member), int(stop_step)))
+
+    def set_tiling(self, member, chunk, warp16x4=True):
+        _check(lib().fslbm_batch_set_tiling(self.handle, int(member), int(chunk), int(bool(warp16x4))))
+
+    def load_tiling(self, path):
+        _check(lib().fslbm_batch_load_tiling(self.handle, os.fsencode(path)))
+
+    def autotune(self, trial_steps=20, path=None):
+        """Per-size-class tiling timed on this batch (state restored afterwards); with `path`
+        the table is also written there as JSON and returned as a dict."""
+        _check(lib().fslbm_batch_autotune(self.handle, int(trial_steps),
+                                          os.fsencode(path) if path else None))
+        if path:
+            import json
+            with open(path) as f:
+                return json.load(f)["classes"]
+        return None
 
     def elapsed_ms(self):
         ms = ctypes.c_double()

@@ -8,8 +8,11 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
+
+#include <dlfcn.h>
 
 #include "internal.h"
 
@@ -164,7 +167,7 @@ struct fslbm_solve {
   // FP32 column-pair kernel (even d1): tile height, persistent grid, two maps per buffer
   bool use2 = false;
   int ty2 = 32, grid2 = 0, packed2 = 1;
-  std::vector<int> tile_warps;     // per column-pair tile: batched-kernel warps (16 x 4 cells) holding fluid
+  std::vector<int> tile_warps[2];  // per column-pair tile: warps holding fluid, [0] 32 x 2, [1] 16 x 4
   CUtensorMap maps2p[2], maps2u[2];
   DevCounters* d_counters = nullptr;
   fslbm_monitor* d_log = nullptr;
@@ -285,20 +288,23 @@ static int configure_kernel(fslbm_solve* s) {
   const char* ep = std::getenv("FSLBM_PACKED");
   s->packed2 = (ep && std::atoi(ep) == 0) ? 0 : 1;
   const std::vector<int2> tiles = fluid_tiles(s, s->use2 ? s->ty2 : kTY);
-  s->tile_warps.clear();
+  s->tile_warps[0].clear();
+  s->tile_warps[1].clear();
   if (s->use2)
-    for (const int2 org : tiles) {
-      int warps = 0;
-      for (int w = 0; w < s->ty2 / 2; ++w) {       // warp w: columns 16*(w%2).., rows 4*(w/2)..
-        const int x0 = org.x + 16 * (w & 1), y0 = org.y + 4 * (w >> 1);
-        bool any = false;
-        for (int y = y0; y < std::min(y0 + 4, s->ly) && !any; ++y)
-          for (int x = x0; x < std::min(x0 + 16, s->lxp) && !any; ++x)
-            any = s->mask[size_t(y) * s->lxp + x] == 0;
-        warps += any;
+    for (const int2 org : tiles)
+      for (int shape = 0; shape < 2; ++shape) {
+        const int wx = shape ? 16 : 32, wy = shape ? 4 : 2;
+        int warps = 0;
+        for (int w = 0; w < s->ty2 / 2; ++w) {
+          const int x0 = org.x + (shape ? 16 * (w & 1) : 0), y0 = org.y + (shape ? 4 * (w >> 1) : 2 * w);
+          bool any = false;
+          for (int y = y0; y < std::min(y0 + wy, s->ly) && !any; ++y)
+            for (int x = x0; x < std::min(x0 + wx, s->lxp) && !any; ++x)
+              any = s->mask[size_t(y) * s->lxp + x] == 0;
+          warps += any;
+        }
+        s->tile_warps[shape].push_back(warps);
       }
-      s->tile_warps.push_back(warps);
-    }
   if (s->d_tiles) {
     ctx_free(s->ctx, s->d_tiles);
     s->bytes_device -= int64_t(s->ntiles) * sizeof(int2);
@@ -1033,8 +1039,10 @@ struct fslbm_batch {
   std::vector<BatchMon> h_mons;
   std::vector<int2> h_items;
   int nitems = 0, grid = 0, packed = 1;
-  int chunk = 64;                  // streamwise planes per work item (FSLBM_BATCH_CHUNK)
-  int chunk_used = 64;             // after shortening for small batches
+  // per member tiling: streamwise planes per work item and warp shape (16 x 4 or 32 x 2),
+  // from the tuning table by size class, else 64 (FSLBM_BATCH_CHUNK) and 16 x 4
+  std::vector<int> m_chunk, m_w4;
+  int shrink = 1;                  // chunk divisor for batches with fewer than 2 items per SM
   cudaGraphExec_t exec2 = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
@@ -1056,8 +1064,8 @@ static void free_batch(fslbm_batch* b) {
 // Work of one (tile, chunk) item of the column-pair kernel, for ordering the items: planes
 // marched (the chunk plus the 2R pipeline planes) times the tile's warps that compute plus two
 // for the pipeline's fixed cost.
-static int64_t item_cost(const fslbm_solve* s, int tile, int nout) {
-  return int64_t(nout + 4 * s->prm.d1) * (s->tile_warps[tile] + 2);
+static int64_t item_cost(const fslbm_solve* s, int tile, int nout, int w16x4) {
+  return int64_t(nout + 4 * s->prm.d1) * (s->tile_warps[w16x4 ? 1 : 0][tile] + 2);
 }
 
 // Streamwise chunks of a member: about `chunk` planes each, at least 4*d1 planes.
@@ -1077,15 +1085,16 @@ static int batch_upload(fslbm_batch* b) {
   const bool build_items = b->h_items.empty();
   struct Item { int64_t cost; int2 it; };
   std::vector<Item> items;
+  auto eff_chunk = [&](int i) { return std::max(4 * b->members[i]->prm.d1, b->m_chunk[i] / b->shrink); };
   if (build_items) {
     // shorter chunks while there are fewer than two items per SM (few or small members)
-    auto count = [&](int chunk) {
+    auto count = [&]() {
       int64_t c = 0;
-      for (fslbm_solve* s : b->members) c += int64_t(s->ntiles) * member_chunks(s, chunk);
+      for (int i = 0; i < n; ++i) c += int64_t(b->members[i]->ntiles) * member_chunks(b->members[i], eff_chunk(i));
       return c;
     };
-    b->chunk_used = b->chunk;
-    while (b->chunk_used > 8 && count(b->chunk_used) < 2 * b->ctx->sm_count) b->chunk_used /= 2;
+    b->shrink = 1;
+    while (b->shrink < 64 && count() < 2 * b->ctx->sm_count) b->shrink *= 2;
   }
   for (int i = 0; i < n; ++i) {
     fslbm_solve* s = b->members[i];
@@ -1095,16 +1104,16 @@ static int batch_upload(fslbm_batch* b) {
     a.tiles = s->d_tiles; a.mask = s->d_mask; a.colcoef = s->d_colcoef;
     a.err = b->d_tickets + 2;        // one flag for the whole batch
     fill_constants(s, a);
-    const int nch = member_chunks(s, b->chunk_used);
+    const int nch = member_chunks(s, eff_chunk(i));
     const long long stop_at = b->stop[i] >= 0 ? (long long)b->stop[i] : LLONG_MAX;
     CUDA_TRY(fill_batch_member(b->h_members.data() + mbytes * i, s->maps2p, s->maps2u, a,
                                s->state[0], s->state[1], s->d_gauge, &s->d_counters->steps,
-                               stop_at, s->prm.monitor_every, s->cur, nch));
+                               stop_at, s->prm.monitor_every, s->cur, nch, b->m_w4[i]));
     if (build_items)
       for (int c = 0; c < nch; ++c) {
         const int nout = int((long long)s->L * (c + 1) / nch - (long long)s->L * c / nch);
         for (int t = 0; t < s->ntiles; ++t)
-          items.push_back({item_cost(s, t, nout), make_int2(i, c * s->ntiles + t)});
+          items.push_back({item_cost(s, t, nout, b->m_w4[i]), make_int2(i, c * s->ntiles + t)});
       }
     BatchMon& m = b->h_mons[i];
     std::memset(&m, 0, sizeof m);
@@ -1148,6 +1157,87 @@ static cudaError_t batch_enqueue_one(fslbm_batch* b, int parity, cudaStream_t st
   return launch_batch_monitor(b->d_mons, int(b->members.size()), parity ^ 1, b->d_tickets, st);
 }
 
+// ------------------------------------------------------------------------------------------
+// batch tiling by size class: table, autotuner
+// ------------------------------------------------------------------------------------------
+// Size class of a member: 32-wide column tiles across x and y, and the streamwise length
+// rounded up to a power of two ("TXxTY:L<log2>"); members of a class share chunk and warp shape.
+static std::string class_key(const fslbm_solve* s) {
+  int lb = 0;
+  while ((1 << lb) < s->L) ++lb;
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "%dx%d:L%d", (s->lxp + kTX - 1) / kTX, (s->ly + 31) / 32, lb);
+  return buf;
+}
+
+struct Tiling { int chunk = 64, w16x4 = 1; double ms = 0; };
+using TilingTable = std::map<std::string, Tiling>;
+
+static bool write_tiling(const char* path, const TilingTable& t) {
+  FILE* f = std::fopen(path, "wt");
+  if (!f) return false;
+  std::fprintf(f, "{\n  \"format\": \"fslbm batch tiling 1\",\n  \"classes\": {");
+  bool first = true;
+  for (const auto& kv : t) {
+    std::fprintf(f, "%s\n    \"%s\": {\"chunk\": %d, \"warp16x4\": %d, \"trial_ms\": %.4f}",
+                 first ? "" : ",", kv.first.c_str(), kv.second.chunk, kv.second.w16x4, kv.second.ms);
+    first = false;
+  }
+  std::fprintf(f, "\n  }\n}\n");
+  return std::fclose(f) == 0;
+}
+
+// Reads the table written by write_tiling: every `"<key>": {"chunk": N, "warp16x4": M` entry.
+static bool read_tiling(const char* path, TilingTable& t) {
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return false;
+  std::string s;
+  char buf[4096];
+  size_t n;
+  while ((n = std::fread(buf, 1, sizeof buf, f)) > 0) s.append(buf, n);
+  std::fclose(f);
+  size_t pos = 0;
+  while ((pos = s.find("{\"chunk\":", pos)) != std::string::npos) {
+    const size_t q1 = s.rfind('"', s.rfind(':', pos));
+    const size_t q0 = q1 == std::string::npos ? q1 : s.rfind('"', q1 - 1);
+    Tiling v;
+    if (q0 != std::string::npos &&
+        std::sscanf(s.c_str() + pos, "{\"chunk\": %d, \"warp16x4\": %d", &v.chunk, &v.w16x4) == 2 &&
+        v.chunk >= 4)
+      t[s.substr(q0 + 1, q1 - q0 - 1)] = v;
+    pos += 9;
+  }
+  return true;
+}
+
+static void apply_tiling(fslbm_batch* b, const TilingTable& t) {
+  for (size_t i = 0; i < b->members.size(); ++i) {
+    auto it = t.find(class_key(b->members[i]));
+    if (it == t.end()) continue;
+    b->m_chunk[i] = it->second.chunk;
+    b->m_w4[i] = it->second.w16x4 ? 1 : 0;
+  }
+  b->h_items.clear();              // rebuild the work items
+}
+
+// The tuning table used when a batch is created: FSLBM_BATCH_TUNING, else batch_tiling.json next
+// to this library (a table measured on a B200 ships with the package), else none.
+static void default_tiling(fslbm_batch* b) {
+  std::string path;
+  if (const char* e = std::getenv("FSLBM_BATCH_TUNING")) {
+    path = e;
+  } else {
+    Dl_info info;
+    if (dladdr(reinterpret_cast<void*>(&fslbm_version), &info) && info.dli_fname) {
+      path = info.dli_fname;
+      const size_t slash = path.rfind('/');
+      path = (slash == std::string::npos ? std::string(".") : path.substr(0, slash)) + "/batch_tiling.json";
+    }
+  }
+  TilingTable t;
+  if (!path.empty() && read_tiling(path.c_str(), t)) apply_tiling(b, t);
+}
+
 extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, int n, fslbm_batch** out) {
   if (!ctx || !out || n < 1 || !solves) return fslbm_set_error(FSLBM_ERR_ARG, "batch_create: bad argument");
   auto* b = new fslbm_batch;
@@ -1160,15 +1250,19 @@ extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, in
     }
     b->members.push_back(solves[i]);
     b->stop.push_back(-1);
+    b->m_chunk.push_back(64);
+    b->m_w4.push_back(1);
     fast = fast && solves[i]->use2 && solves[i]->ty2 == 32 && solves[i]->prm.d1 == 2 &&
            solves[i]->dtype == solves[0]->dtype;
   }
   b->fast = fast;
-  if (const char* ec = std::getenv("FSLBM_BATCH_CHUNK")) b->chunk = std::max(8, std::atoi(ec));
-  // packed FP32x2 pair arithmetic (measured 2 % faster than scalar pairs in the batched kernel
-  // despite a small register spill); FSLBM_BATCH_PACKED=0 selects scalar pairs
+  default_tiling(b);
+  if (const char* ec = std::getenv("FSLBM_BATCH_CHUNK"))
+    for (int& c : b->m_chunk) c = std::max(8, std::atoi(ec));
+  // scalar pair arithmetic: with both warp shapes in one kernel the packed FP32x2 variant spills
+  // registers (FSLBM_BATCH_PACKED=1 selects it, for comparisons)
   const char* ebp = std::getenv("FSLBM_BATCH_PACKED");
-  b->packed = (ebp && std::atoi(ebp) == 0) ? 0 : 1;
+  b->packed = (ebp && std::atoi(ebp) == 1) ? 1 : 0;
   cudaError_t e = cudaSetDevice(ctx->device);
   if (!e && fast) e = batch_prepare(solves[0]->dtype);
   if (!e && fast) e = ctx_alloc(ctx, &b->d_members, batch_member_bytes() * n);
@@ -1269,5 +1363,137 @@ extern "C" int fslbm_batch_sync(fslbm_batch* b) {
 extern "C" int fslbm_batch_elapsed(fslbm_batch* b, double* ms) {
   if (!b || !ms) return fslbm_set_error(FSLBM_ERR_ARG, "batch_elapsed: null argument");
   *ms = b->last_ms;
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_batch_set_tiling(fslbm_batch* b, int member, int chunk, int warp16x4) {
+  if (!b || member < 0 || member >= int(b->members.size()) || chunk < 1)
+    return fslbm_set_error(FSLBM_ERR_ARG, "batch_set_tiling: bad batch, member or chunk");
+  b->m_chunk[member] = chunk;
+  b->m_w4[member] = warp16x4 ? 1 : 0;
+  b->h_items.clear();
+  return FSLBM_OK;
+}
+
+extern "C" int fslbm_batch_load_tiling(fslbm_batch* b, const char* path) {
+  if (!b || !path) return fslbm_set_error(FSLBM_ERR_ARG, "batch_load_tiling: null argument");
+  TilingTable t;
+  if (!read_tiling(path, t)) return fslbm_set_error(FSLBM_ERR_IO, "batch_load_tiling: cannot read %s", path);
+  apply_tiling(b, t);
+  return FSLBM_OK;
+}
+
+// Times candidate tilings on the batch itself: first one tiling for all members (chunks 32, 64,
+// 128 planes, both warp shapes), then per size class, largest first, the neighbouring chunks and
+// the other warp shape while the other classes keep theirs; a change is kept only when it is at
+// least 0.3 % faster (each timing is the better of two trials). The members' fields, step
+// counts, monitor logs and gauges are restored afterwards.
+extern "C" int fslbm_batch_autotune(fslbm_batch* b, int trial_steps, const char* path) {
+  if (!b || trial_steps < 1) return fslbm_set_error(FSLBM_ERR_ARG, "batch_autotune: bad argument");
+  if (!b->fast)
+    return fslbm_set_error(FSLBM_ERR_STATE, "batch_autotune: the members do not use the batched kernel");
+  for (fslbm_solve* s : b->members)
+    if (!s->fields_set) return fslbm_set_error(FSLBM_ERR_STATE, "batch_autotune: a member has no fields");
+  CUDA_TRY(cudaSetDevice(b->ctx->device));
+  cudaStream_t st = b->ctx->stream;
+  const int n = int(b->members.size());
+  // snapshot
+  struct Snap { void* state = nullptr; DevCounters c{}; double gauge = 0; int64_t steps = 0, launches = 0, drained = 0; int cur = 0; };
+  std::vector<Snap> snap(n);
+  CUDA_TRY(cudaStreamSynchronize(st));
+  int rc = FSLBM_OK;
+  for (int i = 0; i < n && !rc; ++i) {
+    fslbm_solve* s = b->members[i];
+    const size_t bytes = 4 * field_stride(s) * s->es;
+    Snap& q = snap[i];
+    q.steps = s->steps; q.cur = s->cur; q.launches = s->launches; q.drained = s->drained;
+    cudaError_t e = ctx_alloc(b->ctx, &q.state, bytes);
+    if (!e) e = cudaMemcpyAsync(q.state, s->state[s->cur], bytes, cudaMemcpyDeviceToDevice, st);
+    if (!e) e = cudaMemcpyAsync(&q.c, s->d_counters, sizeof q.c, cudaMemcpyDeviceToHost, st);
+    if (!e) e = cudaMemcpyAsync(&q.gauge, s->d_gauge, sizeof q.gauge, cudaMemcpyDeviceToHost, st);
+    if (e) rc = fslbm_set_error(FSLBM_ERR_CUDA, "batch_autotune: snapshot: %s", cudaGetErrorString(e));
+  }
+  if (!rc && cudaStreamSynchronize(st)) rc = fslbm_set_error(FSLBM_ERR_CUDA, "batch_autotune: snapshot sync");
+  const std::vector<int64_t> stops = b->stop;
+  for (int64_t& x : b->stop) x = -1;
+  // classes, largest first
+  std::map<std::string, std::vector<int>> cls;
+  for (int i = 0; i < n; ++i) cls[class_key(b->members[i])].push_back(i);
+  std::vector<std::pair<int64_t, std::string>> order;
+  for (const auto& kv : cls) {
+    int64_t cells = 0;
+    for (int i : kv.second) cells += int64_t(b->members[i]->lx) * b->members[i]->ly * b->members[i]->L;
+    order.push_back({-cells, kv.first});
+  }
+  std::sort(order.begin(), order.end());
+  auto trial = [&](double* ms) -> int {
+    double best = 1e30;
+    for (int rep = 0; rep < 2; ++rep) {
+      if (int r = fslbm_batch_step(b, 2, 1)) return r;       // warm: items, graph
+      if (int r = fslbm_batch_sync(b)) return r;
+      if (int r = fslbm_batch_step(b, trial_steps, 1)) return r;
+      if (int r = fslbm_batch_sync(b)) return r;
+      best = std::min(best, b->last_ms);
+    }
+    *ms = best;
+    return FSLBM_OK;
+  };
+  auto set = [&](const std::vector<int>& mem, int c, int w) {
+    for (int i : mem) { b->m_chunk[i] = c; b->m_w4[i] = w; }
+    b->h_items.clear();
+  };
+  std::vector<int> all(n);
+  for (int i = 0; i < n; ++i) all[i] = i;
+  Tiling glob;
+  glob.ms = 1e30;
+  for (int w = 1; w >= 0 && !rc; --w)
+    for (int c : {32, 64, 128}) {
+      set(all, c, w);
+      double ms = 0;
+      if ((rc = trial(&ms))) break;
+      if (ms < glob.ms) { glob.ms = ms; glob.chunk = c; glob.w16x4 = w; }
+    }
+  set(all, glob.chunk, glob.w16x4);
+  double cur_ms = glob.ms;
+  TilingTable table;
+  for (size_t oi = 0; oi < order.size() && !rc; ++oi) {
+    const std::vector<int>& mem = cls[order[oi].second];
+    int maxL = 0;
+    for (int i : mem) maxL = std::max(maxL, b->members[i]->L);
+    Tiling best = glob;
+    best.ms = cur_ms;
+    const std::pair<int, int> cands[] = {{glob.chunk / 2, glob.w16x4}, {glob.chunk * 2, glob.w16x4},
+                                         {glob.chunk, 1 - glob.w16x4}};
+    for (const auto& cw : cands) {
+      if (cw.first < 16 || (cw.first / 2 >= maxL && cw.first > glob.chunk)) continue;
+      set(mem, cw.first, cw.second);
+      double ms = 0;
+      if ((rc = trial(&ms))) break;
+      if (ms < best.ms * 0.997) { best.ms = ms; best.chunk = cw.first; best.w16x4 = cw.second; }
+    }
+    set(mem, best.chunk, best.w16x4);
+    cur_ms = best.ms;
+    table[order[oi].second] = best;
+  }
+  // restore
+  b->stop = stops;
+  CUDA_TRY(cudaStreamSynchronize(st));
+  for (int i = 0; i < n; ++i) {
+    fslbm_solve* s = b->members[i];
+    Snap& q = snap[i];
+    if (!q.state) continue;
+    s->steps = q.steps; s->cur = q.cur; s->launches = q.launches; s->drained = q.drained;
+    CUDA_TRY(cudaMemcpyAsync(s->state[s->cur], q.state, 4 * field_stride(s) * s->es,
+                             cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(s->d_counters, &q.c, sizeof q.c, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(s->d_gauge, &q.gauge, sizeof q.gauge, cudaMemcpyHostToDevice, st));
+    ctx_free(b->ctx, q.state);
+  }
+  CUDA_TRY(cudaMemsetAsync(b->d_tickets + 2, 0, sizeof(unsigned), st));
+  CUDA_TRY(cudaStreamSynchronize(st));             // host snapshots stay alive until copied
+  b->h_items.clear();
+  if (rc) return rc;
+  if (path && !write_tiling(path, table))
+    return fslbm_set_error(FSLBM_ERR_IO, "batch_autotune: cannot write %s", path);
   return FSLBM_OK;
 }

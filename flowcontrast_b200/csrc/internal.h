@@ -83,7 +83,7 @@ size_t batch_member_bytes();
 cudaError_t fill_batch_member(void* dst, const CUtensorMap* map_p, const CUtensorMap* map_u,
                               const StepLaunch& a, void* state0, void* state1,
                               const double* gauge_slot, const long long* steps, long long stop_at,
-                              int monitor_every, int cur0, int nchunks);
+                              int monitor_every, int cur0, int nchunks, int w16x4);
 // items: nitems (member, item of the member) pairs; tickets: two counters (per step parity)
 // that start at zero; the bookkeeping launch resets the one its step used.
 cudaError_t launch_batch_step(int dtype, const void* members, const int2* items, int nitems,

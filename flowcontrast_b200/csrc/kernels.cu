@@ -292,7 +292,7 @@ size_t batch_member_bytes() { return sizeof(BatchMember); }
 cudaError_t fill_batch_member(void* dst, const CUtensorMap* mp, const CUtensorMap* mu,
                               const StepLaunch& a, void* state0, void* state1,
                               const double* gauge_slot, const long long* steps, long long stop_at,
-                              int monitor_every, int cur0, int nchunks) {
+                              int monitor_every, int cur0, int nchunks, int w16x4) {
   BatchMember m;
   std::memset(&m, 0, sizeof m);
   m.map_p[0] = mp[0]; m.map_p[1] = mp[1];
@@ -304,7 +304,7 @@ cudaError_t fill_batch_member(void* dst, const CUtensorMap* mp, const CUtensorMa
   m.k.m = float(a.m); m.k.c0 = float(a.c0); m.k.c1 = float(a.c1); m.k.c2 = float(a.c2);
   m.k.fx = float(a.fx); m.k.fy = float(a.fy); m.k.fz = float(a.fz);
   m.state[0] = state0; m.state[1] = state1;
-  m.gauge_slot = gauge_slot; m.steps = steps; m.stop_at = stop_at;
+  m.gauge_slot = gauge_slot; m.steps = steps; m.stop_at = stop_at; m.w16x4 = w16x4;
   m.monitor_every = monitor_every; m.cur0 = cur0;
   std::memcpy(dst, &m, sizeof m);
   return cudaSuccess;

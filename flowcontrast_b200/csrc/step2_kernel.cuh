@@ -522,6 +522,7 @@ struct alignas(64) BatchMember {
   const double* gauge_slot;    // the member's monitor p2, applied on the step after a monitor
   const long long* steps;      // the member's device step counter
   long long stop_at;           // the member is not stepped once its counter reaches this
+  int w16x4;                   // warp shape of the member's items (16 x 4 instead of 32 x 2)
   int monitor_every;
   int cur0;                    // input buffer at batch parity 0
 };
@@ -563,9 +564,14 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
       s_k = mb.k;
     }
     __syncthreads();
-    if (!step2_march<D1, TY, PK, TE, true>(&mb.map_p[cur], &mb.map_u[cur], s_g, s_k, it.y % ntiles,
-                                     it.y / ntiles, smem, !first))
-      return;
+    // the warp shape is a compile-time choice (a runtime one raises register pressure)
+    const bool ok = mb.w16x4 ? step2_march<D1, TY, PK, TE, true>(&mb.map_p[cur], &mb.map_u[cur], s_g,
+                                                                 s_k, it.y % ntiles, it.y / ntiles,
+                                                                 smem, !first)
+                             : step2_march<D1, TY, PK, TE, false>(&mb.map_p[cur], &mb.map_u[cur], s_g,
+                                                                  s_k, it.y % ntiles, it.y / ntiles,
+                                                                  smem, !first);
+    if (!ok) return;
     first = false;
   }
 }

@@ -187,6 +187,19 @@ int fslbm_batch_elapsed(fslbm_batch* b, double* ms);
  * stop_step (absolute; -1 = no stop), so members with different step budgets share launches;
  * the others keep stepping. */
 int fslbm_batch_set_stop(fslbm_batch* b, int member, int64_t stop_step);
+/* Batch tiling (no reference counterpart). A member's work items span `chunk` streamwise planes
+ * (each chunk re-reads 2*2*d1 halo planes) and use warps of 16 x 4 cells (warp16x4 = 1) or
+ * 32 x 2 cells (0). Members fall in size classes (32-wide tiles across x and y, length rounded
+ * up to a power of two); a batch takes its classes' tiling from the table named by the
+ * FSLBM_BATCH_TUNING environment variable, else from batch_tiling.json next to the library,
+ * else 64 planes and 16 x 4 warps. */
+int fslbm_batch_set_tiling(fslbm_batch* b, int member, int chunk, int warp16x4);
+int fslbm_batch_load_tiling(fslbm_batch* b, const char* path);
+/* Autotuner: times each size class's candidate tilings (chunks 16..256, both warp shapes) on the
+ * batch itself, trial_steps steps per candidate, keeps the fastest per class, restores every
+ * member's fields, step count, monitor log and gauge, and writes the table to `path` (JSON) if
+ * not NULL. Needs members on the batched kernel (FP32 or FP16 storage, d1 = 2). */
+int fslbm_batch_autotune(fslbm_batch* b, int trial_steps, const char* path);
 
 /* ---- served solves: a request loop with continuous batching (no reference counterpart) ----
  * The server owns a context on `device` and a worker thread. Requests are admitted in arrival

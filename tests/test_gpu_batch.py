@@ -101,3 +101,44 @@ def test_batch_member_stops(built, ctx):
     b.close()
     for s in members:
         s.close()
+
+
+def test_autotune_restores_state_and_keeps_results(built, ctx, tmp_path):
+    """The autotuner times tilings on the batch itself and restores every member; tiling never
+    changes results, so the tuned batch still equals each member stepped alone, and a saved
+    table loads into another batch."""
+    import json
+    fb = built
+    specs = member_specs(n=5, seed=21)
+    steps = 30
+    alone = []
+    for sp in specs:
+        s = make_member(fb, ctx, sp)
+        s.step(steps)
+        s.sync()
+        alone.append((s.get_fields(np.float32), s.monitor_log()))
+        s.close()
+    members = [make_member(fb, ctx, sp) for sp in specs]
+    b = fb.Batch(ctx, members)
+    path = str(tmp_path / "tiling.json")
+    table = b.autotune(trial_steps=4, path=path)
+    assert table and all(set(v) >= {"chunk", "warp16x4"} for v in table.values())
+    assert json.load(open(path))["format"] == "fslbm batch tiling 1"
+    for s in members:
+        assert s.info()["steps"] == 0 and s.monitor_log() == []
+    b.step(steps)
+    b.sync()
+    for s, (want, wlog) in zip(members, alone):
+        assert np.array_equal(s.get_fields(np.float32), want)
+        assert [r["q1"] for r in s.monitor_log()] == [r["q1"] for r in wlog]
+    b.close()
+    again = [make_member(fb, ctx, sp) for sp in specs]
+    b2 = fb.Batch(ctx, again)
+    b2.load_tiling(path)
+    b2.step(steps)
+    b2.sync()
+    for s, (want, _) in zip(again, alone):
+        assert np.array_equal(s.get_fields(np.float32), want)
+    b2.close()
+    for s in members + again:
+        s.close()
