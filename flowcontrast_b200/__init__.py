@@ -42,17 +42,20 @@ class Params(ctypes.Structure):
     _fields_ = [("tblend", ctypes.c_double), ("pin", ctypes.c_double),
                 ("nu", ctypes.c_double), ("d1", ctypes.c_int), ("delta", ctypes.c_int),
                 ("blend", ctypes.c_double), ("monitor_every", ctypes.c_int),
-                ("force", ctypes.c_double * 3)]
+                ("force", ctypes.c_double * 3), ("fd_order", ctypes.c_int)]
 
     @classmethod
     def make(cls, tblend=1.0, pin=0.003, nu=0.004006, d1=2, delta=1, blend=0.0,
-             monitor_every=50, force=(0.0, 0.0, 0.0)):
-        """Defaults are pipe.m's param.txt (pipe.m:68) and the reference's 50-step monitor."""
-        return cls(tblend, pin, nu, d1, delta, blend, monitor_every, (ctypes.c_double * 3)(*force))
+             monitor_every=50, force=(0.0, 0.0, 0.0), fd_order=0):
+        """Defaults are pipe.m's param.txt (pipe.m:68) and the reference's 50-step monitor;
+        fd_order 0 is the reference's active 4<->2 corrector blend."""
+        return cls(tblend, pin, nu, d1, delta, blend, monitor_every, (ctypes.c_double * 3)(*force),
+                   int(fd_order))
 
     def as_dict(self):
         return dict(tblend=self.tblend, pin=self.pin, nu=self.nu, d1=self.d1, delta=self.delta,
-                    blend=self.blend, monitor_every=self.monitor_every, force=tuple(self.force))
+                    blend=self.blend, monitor_every=self.monitor_every, force=tuple(self.force),
+                    fd_order=self.fd_order)
 
 
 class Monitor(ctypes.Structure):
@@ -172,6 +175,7 @@ def lib():
             "fslbm_solve_init_poiseuille": ([_vp, ctypes.c_double, ctypes.c_double, _i,
                                              ctypes.c_double, ctypes.c_uint64], _i),
             "fslbm_solve_footprint": ([ctypes.POINTER(Domain), _i, ctypes.POINTER(ctypes.c_int64)], _i),
+            "fslbm_fd_coefficients": ([_i, ctypes.c_double, _i, _vp, ctypes.POINTER(_i)], _i),
             "fslbm_server_create": ([_i, ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)], _i),
             "fslbm_server_destroy": ([_vp], _i),
             "fslbm_server_submit": ([_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)], _i),
@@ -562,3 +566,11 @@ class Server:
 
     def __exit__(self, *a):
         self.close()
+
+
+def fd_coefficients(order, blend=0.0, dtype=F64):
+    """Corrector coefficients c0..cK of `order` as a solve of `dtype` uses them."""
+    c = np.zeros(9)
+    k = ctypes.c_int()
+    _check(lib().fslbm_fd_coefficients(int(order), float(blend), int(dtype), _ptr(c), ctypes.byref(k)))
+    return c[:k.value + 1]

@@ -150,6 +150,7 @@ struct fslbm_solve {
   int lx = 0, ly = 0, L = 0, lxp = 0, d2 = 10;
   double radius = 0, cx = 0, cy = 0;
   bool from_mask = false;          // geometry given as a mask (else the analytic circle)
+  int K = 2;                       // corrector taps of prm.fd_order
   int dtype = FSLBM_F32;
   size_t es = 4;
   fslbm_params prm{};
@@ -207,8 +208,12 @@ static void elapsed_if_recorded(cudaEvent_t a, cudaEvent_t b, double* out) {
 
 static int validate_params(const fslbm_params* p, int dtype) {
   if (!p) return fslbm_set_error(FSLBM_ERR_ARG, "params: null");
-  if (!step_supported(dtype, p->d1))
-    return fslbm_set_error(FSLBM_ERR_ARG, "params: d1=%d is not supported for dtype %d", p->d1, dtype);
+  double c[9];
+  const int K = fd_coefficients(p->fd_order, p->blend, dtype != FSLBM_F64, c);
+  if (K == 0) return fslbm_set_error(FSLBM_ERR_ARG, "params: unknown corrector order %d", p->fd_order);
+  if (!step_supported(dtype, p->d1, K))
+    return fslbm_set_error(FSLBM_ERR_ARG, "params: d1=%d with corrector order %d is not supported for dtype %d",
+                           p->d1, p->fd_order, dtype);
   if (!std::isfinite(p->tblend) || !std::isfinite(p->pin) || !std::isfinite(p->nu) ||
       !std::isfinite(p->blend))
     return fslbm_set_error(FSLBM_ERR_ARG, "params: non-finite value");
@@ -231,7 +236,7 @@ static int build_tensor_maps(fslbm_solve* s) {
     CUresult r;
     if (!s->use2) {
       int sw, sh, hx, hy;
-      if (!step_box(s->dtype, s->prm.d1, &sw, &sh, &hx, &hy))
+      if (!step_box(s->dtype, s->prm.d1, s->K, &sw, &sh, &hx, &hy))
         return fslbm_set_error(FSLBM_ERR_ARG, "no step kernel for dtype %d d1 %d", s->dtype, s->prm.d1);
       cuuint32_t box[4] = {cuuint32_t(sw), cuuint32_t(sh), 1, 4};
       r = enc(&s->maps[b], dt, 4, s->state[b], dims, strides, box, estr,
@@ -281,8 +286,10 @@ static void choose_chunks(fslbm_solve* s);
 static int configure_kernel(fslbm_solve* s) {
   const char* ek = std::getenv("FSLBM_STEP_KERNEL");
   const char* et = std::getenv("FSLBM_TILE_Y");
-  // FP16 storage exists only in the column-pair kernel
-  s->use2 = step2_supported(s->dtype, s->prm.d1) &&
+  double cf[9];
+  s->K = fd_coefficients(s->prm.fd_order, s->prm.blend, s->dtype != FSLBM_F64, cf);
+  // FP16 storage exists only in the column-pair kernel, which has the 2-tap corrector
+  s->use2 = step2_supported(s->dtype, s->prm.d1) && s->K == 2 &&
             (s->dtype == FSLBM_F16 || !(ek && std::atoi(ek) == 1));
   s->ty2 = (et && std::atoi(et) == 16) ? 16 : 32;
   const char* ep = std::getenv("FSLBM_PACKED");
@@ -323,7 +330,7 @@ static int configure_kernel(fslbm_solve* s) {
     nch = std::min(nch, std::max(1, s->L / (4 * s->prm.d1)));
     s->grid2 = s->ntiles * nch;
   } else {
-    CUDA_TRY(step_prepare(s->dtype, s->prm.d1));
+    CUDA_TRY(step_prepare(s->dtype, s->prm.d1, s->K));
     choose_chunks(s);
   }
   return build_tensor_maps(s);
@@ -357,11 +364,11 @@ static std::vector<ColCoef<TC>> column_coefs(const fslbm_solve* s) {
 // Picks the streamwise chunking: minimises waves * (chunk + 2R) over chunk counts.
 static void choose_chunks(fslbm_solve* s) {
   int occ = 1;
-  const size_t smem = step_smem_bytes(s->dtype, s->prm.d1);
+  const size_t smem = step_smem_bytes(s->dtype, s->prm.d1, s->K);
   occ = s->dtype == FSLBM_F64 ? 1 : 2;
   if (smem * occ > 227 * 1024) occ = 1;
   const int slots = std::max(1, s->ctx->sm_count * occ);
-  const int R = 2 * s->prm.d1;
+  const int R = s->K * s->prm.d1;
   double best = 1e300;
   int best_n = 1;
   for (int n = 1; n <= s->L; ++n) {
@@ -406,7 +413,8 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
   if (rc) return rc;
   if (dom->lx < 3 || dom->ly < 3 || dom->lz < 1)
     return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: box %dx%dx%d too small", dom->lx, dom->ly, dom->lz);
-  const int R = 2 * prm->d1;
+  double cf[9];
+  const int R = fd_coefficients(prm->fd_order, prm->blend, dtype != FSLBM_F64, cf) * prm->d1;
   if (dom->lz < std::max(R, 1) + 1)
     return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: streamwise period %d shorter than the stencil reach %d",
                            dom->lz, R + 1);
@@ -512,7 +520,7 @@ extern "C" int fslbm_solve_set_params(fslbm_solve* s, const fslbm_params* prm) {
   if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "set_params: null solve");
   int rc = validate_params(prm, s->dtype);
   if (rc) return rc;
-  const bool d1_changed = prm->d1 != s->prm.d1;
+  const bool d1_changed = prm->d1 != s->prm.d1 || prm->fd_order != s->prm.fd_order;
   s->prm = *prm;
   if (d1_changed) {
     CUDA_TRY(cudaSetDevice(s->ctx->device));
@@ -650,9 +658,7 @@ static void fill_constants(const fslbm_solve* s, StepLaunch& a) {
     a.pin = float(p.pin);
     a.dtddy = nu - 0.16666666f;
     a.m = float(1.0 / double(float(p.d1 * p.d1)));
-    a.c0 = -6.0f - 1.5f * blend;
-    a.c1 = 1.0f + 0.3333333333f * blend;
-    a.c2 = -0.0833333333f * blend;
+    (void)blend;
     a.fx = float(p.force[0]); a.fy = float(p.force[1]); a.fz = float(p.force[2]);
   } else {
     a.tb = p.tblend;
@@ -660,11 +666,13 @@ static void fill_constants(const fslbm_solve* s, StepLaunch& a) {
     a.pin = p.pin;
     a.dtddy = p.nu - 0.16666666;
     a.m = 1.0 / double(p.d1 * p.d1);
-    a.c0 = -6.0 - 1.5 * p.blend;
-    a.c1 = 1.0 + 0.3333333333 * p.blend;
-    a.c2 = -0.0833333333 * p.blend;
     a.fx = p.force[0]; a.fy = p.force[1]; a.fz = p.force[2];
   }
+  // corrector coefficients of the order (FSLBM.cu:177-232), formed as the reference forms them
+  double c[9];
+  a.K = fd_coefficients(p.fd_order, p.blend, s->dtype != FSLBM_F64, c);
+  a.c0 = c[0]; a.c1 = c[1]; a.c2 = c[2];
+  for (int j = 0; j < 6; ++j) a.ch[j] = c[3 + j];
 }
 
 static int enqueue_steps(fslbm_solve* s, int64_t nsteps) {

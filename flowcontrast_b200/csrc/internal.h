@@ -31,13 +31,16 @@ struct StepLaunch {
   unsigned* err;
   DevCounters* counters;     // steps incremented by the launch
   long long step_no;         // the time step this launch computes (1-based; rounding seed)
+  int K;                     // corrector taps (2: the reference's order 2<->4 blend)
   // constants in double; converted to the compute type by the launcher
   double tb, cc, pin, dtddy, m, c0, c1, c2, fx, fy, fz;
+  double ch[6];              // corrector coefficients c3..c8
 };
 
-size_t step_smem_bytes(int dtype, int d1);
-bool step_supported(int dtype, int d1);
-cudaError_t step_prepare(int dtype, int d1);   // sets the dynamic shared memory attribute
+// One-column kernel for (storage type, d1, corrector taps K).
+size_t step_smem_bytes(int dtype, int d1, int K);
+bool step_supported(int dtype, int d1, int K);
+cudaError_t step_prepare(int dtype, int d1, int K);   // sets the dynamic shared memory attribute
 cudaError_t launch_step(const StepLaunch& a, cudaStream_t st);
 
 // FP32 column-pair kernel (even d1): two tensor maps per input state (p box with a one-cell
@@ -114,7 +117,11 @@ cudaError_t launch_convert_out(int dtype, const void* state, void* dst, int dst_
 
 namespace fslbm {
 // TMA box of the step kernel for (dtype, d1): slot row length, rows, halos.
-bool step_box(int dtype, int d1, int* sw, int* sh, int* hx, int* hy);
+bool step_box(int dtype, int d1, int K, int* sw, int* sh, int* hx, int* hy);
+// Corrector coefficients c0..c8 of an order (0/4: the reference's 4<->2 blend, 6: 6<->4,
+// 8: 8<->6, 10/12/14: fixed), formed in FP32 (fp32 != 0) or FP64 as the reference forms its
+// active set. Returns the tap count K, 0 for an unknown order.
+int fd_coefficients(int order, double blend, int fp32, double* c);
 // Gathers the YZ plane x = idx (kind 0, out [4][L][ly]) or the XY plane z = idx
 // (kind 1, out [4][ly][lx]) of the four fields as FP32 into device memory.
 cudaError_t launch_gather_plane(int dtype, const void* state, int lx, int lxp, int ly, int L,

@@ -18,10 +18,10 @@ __device__ __forceinline__ double to_d(__half x) { return double(__half2float(x)
 // ------------------------------------------------------------------------------------------
 // step dispatch
 // ------------------------------------------------------------------------------------------
-template <class TS, int D1>
+template <class TS, int D1, int K>
 static cudaError_t launch_step_t(const StepLaunch& a, cudaStream_t st) {
   using TC = typename Compute<TS>::type;
-  using Tl = StepTile<TS, D1>;
+  using Tl = StepTile<TS, D1, K>;
   StepGeom g;
   g.lxp = a.lxp; g.ly = a.ly; g.L = a.L;
   g.ntiles = a.ntiles; g.chunk = a.chunk;
@@ -31,61 +31,52 @@ static cudaError_t launch_step_t(const StepLaunch& a, cudaStream_t st) {
   StepConst<TC> k;
   k.tb = TC(a.tb); k.cc = TC(a.cc); k.pin = TC(a.pin); k.dtddy = TC(a.dtddy); k.m = TC(a.m);
   k.c0 = TC(a.c0); k.c1 = TC(a.c1); k.c2 = TC(a.c2);
+  for (int j = 0; j < 6; ++j) k.ch[j] = TC(a.ch[j]);
   k.fx = TC(a.fx); k.fy = TC(a.fy); k.fz = TC(a.fz);
   const int grid = a.ntiles * a.nchunks;
-  fslbm_step_kernel<TS, D1><<<grid, kThreads, Tl::SMEM_BYTES, st>>>(*a.map, g, k);
+  fslbm_step_kernel<TS, D1, K><<<grid, kThreads, Tl::SMEM_BYTES, st>>>(*a.map, g, k);
   return cudaGetLastError();
 }
 
-template <class TS, int D1>
-static cudaError_t prepare_t() {
-  using Tl = StepTile<TS, D1>;
-  return cudaFuncSetAttribute(fslbm_step_kernel<TS, D1>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, int(Tl::SMEM_BYTES));
-}
+// (storage type, d1, corrector taps K) built for the one-column kernel: shared memory holds
+// R + 3 planes of the tile with an R = K*d1 halo, which bounds R at 8 for FP32 and 4 for FP64.
+#define FSLBM_STEP_COMBOS(X)                                                                    \
+  X(FSLBM_F32, float, 1, 2) X(FSLBM_F32, float, 2, 2) X(FSLBM_F32, float, 3, 2)                \
+  X(FSLBM_F32, float, 1, 3) X(FSLBM_F32, float, 1, 4) X(FSLBM_F32, float, 1, 5)                \
+  X(FSLBM_F32, float, 1, 6) X(FSLBM_F32, float, 1, 8) X(FSLBM_F32, float, 2, 3)                \
+  X(FSLBM_F32, float, 2, 4) X(FSLBM_F64, double, 1, 2) X(FSLBM_F64, double, 2, 2)              \
+  X(FSLBM_F64, double, 1, 3) X(FSLBM_F64, double, 1, 4)
 
-template <class TS, int D1> static size_t smem_t() { return StepTile<TS, D1>::SMEM_BYTES; }
-
-bool step_supported(int dtype, int d1) {
-  if (dtype == FSLBM_F32) return d1 >= 1 && d1 <= 3;
-  if (dtype == FSLBM_F64) return d1 >= 1 && d1 <= 2;
-  if (dtype == FSLBM_F16) return d1 == 2;      // column-pair kernel only
+bool step_supported(int dtype, int d1, int K) {
+#define X(DT, TS, D, KK) if (dtype == DT && d1 == D && K == KK) return true;
+  FSLBM_STEP_COMBOS(X)
+#undef X
+  if (dtype == FSLBM_F16) return d1 == 2 && K == 2;   // column-pair kernel only
   return false;
 }
 
-size_t step_smem_bytes(int dtype, int d1) {
-  if (dtype == FSLBM_F32) {
-    if (d1 == 1) return smem_t<float, 1>();
-    if (d1 == 2) return smem_t<float, 2>();
-    if (d1 == 3) return smem_t<float, 3>();
-  } else if (dtype == FSLBM_F64) {
-    if (d1 == 1) return smem_t<double, 1>();
-    if (d1 == 2) return smem_t<double, 2>();
-  }
+size_t step_smem_bytes(int dtype, int d1, int K) {
+#define X(DT, TS, D, KK) if (dtype == DT && d1 == D && K == KK) return StepTile<TS, D, KK>::SMEM_BYTES;
+  FSLBM_STEP_COMBOS(X)
+#undef X
   return 0;
 }
 
-cudaError_t step_prepare(int dtype, int d1) {
-  if (dtype == FSLBM_F32) {
-    if (d1 == 1) return prepare_t<float, 1>();
-    if (d1 == 2) return prepare_t<float, 2>();
-    if (d1 == 3) return prepare_t<float, 3>();
-  } else if (dtype == FSLBM_F64) {
-    if (d1 == 1) return prepare_t<double, 1>();
-    if (d1 == 2) return prepare_t<double, 2>();
-  }
+cudaError_t step_prepare(int dtype, int d1, int K) {
+#define X(DT, TS, D, KK)                                                                        \
+  if (dtype == DT && d1 == D && K == KK)                                                        \
+    return cudaFuncSetAttribute(fslbm_step_kernel<TS, D, KK>,                                   \
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,                    \
+                                int(StepTile<TS, D, KK>::SMEM_BYTES));
+  FSLBM_STEP_COMBOS(X)
+#undef X
   return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_step(const StepLaunch& a, cudaStream_t st) {
-  if (a.dtype == FSLBM_F32) {
-    if (a.d1 == 1) return launch_step_t<float, 1>(a, st);
-    if (a.d1 == 2) return launch_step_t<float, 2>(a, st);
-    if (a.d1 == 3) return launch_step_t<float, 3>(a, st);
-  } else if (a.dtype == FSLBM_F64) {
-    if (a.d1 == 1) return launch_step_t<double, 1>(a, st);
-    if (a.d1 == 2) return launch_step_t<double, 2>(a, st);
-  }
+#define X(DT, TS, D, KK) if (a.dtype == DT && a.d1 == D && a.K == KK) return launch_step_t<TS, D, KK>(a, st);
+  FSLBM_STEP_COMBOS(X)
+#undef X
   return cudaErrorInvalidValue;
 }
 
@@ -596,22 +587,15 @@ cudaError_t launch_profile(int dtype, const void* state, int lxp, int ly, int L,
 
 namespace fslbm {
 
-bool step_box(int dtype, int d1, int* sw, int* sh, int* hx, int* hy) {
-#define FSLBM_BOX(T, D)                                                              \
-  do {                                                                               \
-    using Tl = StepTile<T, D>;                                                       \
-    *sw = Tl::SW; *sh = Tl::SH; *hx = Tl::HX; *hy = Tl::HY;                          \
-    return true;                                                                     \
-  } while (0)
-  if (dtype == FSLBM_F32) {
-    if (d1 == 1) FSLBM_BOX(float, 1);
-    if (d1 == 2) FSLBM_BOX(float, 2);
-    if (d1 == 3) FSLBM_BOX(float, 3);
-  } else if (dtype == FSLBM_F64) {
-    if (d1 == 1) FSLBM_BOX(double, 1);
-    if (d1 == 2) FSLBM_BOX(double, 2);
+bool step_box(int dtype, int d1, int K, int* sw, int* sh, int* hx, int* hy) {
+#define X(DT, TS, D, KK)                                                                        \
+  if (dtype == DT && d1 == D && K == KK) {                                                      \
+    using Tl = StepTile<TS, D, KK>;                                                             \
+    *sw = Tl::SW; *sh = Tl::SH; *hx = Tl::HX; *hy = Tl::HY;                                     \
+    return true;                                                                                \
   }
-#undef FSLBM_BOX
+  FSLBM_STEP_COMBOS(X)
+#undef X
   return false;
 }
 

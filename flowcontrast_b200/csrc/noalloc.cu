@@ -121,6 +121,9 @@ extern "C" int fslbm_step_f32_noalloc(const float* state_in, float* state_out,
                            "preallocated scratch", lx_pitch, ly, kNoallocMaxCells);
   if (prm->d1 != 2)
     return fslbm_set_error(FSLBM_ERR_ARG, "step_f32_noalloc: only d1 = 2 is available (got %d)", prm->d1);
+  if (prm->fd_order != 0 && prm->fd_order != 4)
+    return fslbm_set_error(FSLBM_ERR_ARG, "step_f32_noalloc: corrector order %d needs the one-column kernel; "
+                           "this entry point runs orders 0/4 only", prm->fd_order);
   if (lz < 2 * prm->d1 + 1)
     return fslbm_set_error(FSLBM_ERR_ARG, "step_f32_noalloc: lz = %d shorter than the stencil reach", lz);
   if ((reinterpret_cast<uintptr_t>(state_in) | reinterpret_cast<uintptr_t>(state_out)) % 16)

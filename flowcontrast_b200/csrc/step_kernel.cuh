@@ -23,8 +23,9 @@
 // static per-column sum of W_c c^k over wall neighbours times the centre p, because wall cells
 // hold zero (bcond, FSLBM.cu:290); the mask is extruded along z.
 //
-// Corrector: in-plane taps at +-d1, +-2*d1 come from the ring slot of the output plane, the
-// streamwise taps from a 2R+1 register ring of the thread's own column.
+// Corrector: in-plane taps at +-d1 .. +-K*d1 (K = 2 for the reference's order 2<->4 blend, up to
+// 8 for its order-14 set) come from the ring slot of the output plane, the streamwise taps from a
+// 2R+1 register ring of the thread's own column (R = K*d1).
 #pragma once
 #include <cstdint>
 #include <cuda.h>
@@ -38,8 +39,8 @@ constexpr uint64_t kWaitLimitNs = 2000000000ull;   // 2 s bound on every mbarrie
 
 template <class TS> struct Compute { using type = TS; };
 
-template <class TS, int D1> struct StepTile {
-  static constexpr int R = 2 * D1;                              // farthest corrector tap
+template <class TS, int D1, int K = 2> struct StepTile {
+  static constexpr int R = K * D1;                              // farthest corrector tap
   static constexpr int AL = 16 / int(sizeof(TS));               // elements per 16 bytes
   static constexpr int HX = ((R + AL - 1) / AL) * AL;           // x halo, TMA-aligned start
   static constexpr int HY = R;
@@ -62,6 +63,7 @@ template <class TS, int D1> struct StepTile {
 
 template <class TC> struct StepConst {
   TC tb, cc, pin, dtddy, m, c0, c1, c2, fx, fy, fz;
+  TC ch[6];                // corrector coefficients c3..c8 (orders above 4)
 };
 
 struct StepGeom {
@@ -76,11 +78,11 @@ struct StepGeom {
   long long* step_counter; // device step count, advanced by block 0
 };
 
-template <class TS, int D1>
+template <class TS, int D1, int K = 2>
 __global__ void __launch_bounds__(kThreads, sizeof(TS) == 8 ? 1 : 2)
     fslbm_step_kernel(const __grid_constant__ CUtensorMap tin, const StepGeom g,
                       const StepConst<typename Compute<TS>::type> k) {
-  using Tl = StepTile<TS, D1>;
+  using Tl = StepTile<TS, D1, K>;
   using TC = typename Tl::TC;
   constexpr int R = Tl::R, HX = Tl::HX, HY = Tl::HY, SW = Tl::SW, PL = Tl::PLANE;
   constexpr int S = Tl::S, P = Tl::P, QW = Tl::QW, QN = Tl::QN;
@@ -237,12 +239,17 @@ __global__ void __launch_bounds__(kThreads, sizeof(TS) == 8 ? 1 : 2)
       const TS* po = ring + size_t((i - R) % S) * Tl::SLOT + cidx;
       const TC pc = TC(po[0]);
       const TC uc = ru[R], vc = rv[R], wc = rw[R];
+      // L = c0 u + sum_k c_k (six taps at k*d1), k = 1..K
       auto lap = [&](const TS* f, const TC* rz, TC c) {
-        const TC s1 = TC(f[D1]) + TC(f[-D1]) + TC(f[D1 * SW]) + TC(f[-D1 * SW]) + rz[R + D1] +
-                      rz[R - D1];
-        const TC s2 = TC(f[2 * D1]) + TC(f[-2 * D1]) + TC(f[2 * D1 * SW]) +
-                      TC(f[-2 * D1 * SW]) + rz[2 * R] + rz[0];
-        return c * k.c0 + k.c1 * s1 + k.c2 * s2;
+        TC acc = c * k.c0;
+#pragma unroll
+        for (int kk = 1; kk <= K; ++kk) {
+          const int o = kk * D1;
+          const TC s = TC(f[o]) + TC(f[-o]) + TC(f[o * SW]) + TC(f[-o * SW]) + rz[R + o] + rz[R - o];
+          const TC ck = kk == 1 ? k.c1 : (kk == 2 ? k.c2 : k.ch[kk - 3]);
+          acc += ck * s;
+        }
+        return acc;
       };
       const TC Lu = lap(po + PL, ru, uc), Lv = lap(po + 2 * PL, rv, vc),
                Lw = lap(po + 3 * PL, rw, wc);

@@ -71,6 +71,12 @@ typedef struct {
   double blend;         /* corrector order blend, 0: order 2, 1: order 4 (FSLBM.cu:231) */
   int monitor_every;    /* monitor + pressure gauge period; 50 in the reference (FSLBM.cu:630) */
   double force[3];      /* addition: body force per step on (u,v,w), stored-velocity sign */
+  int fd_order;         /* corrector order (FSLBM.cu:177-232): 0 or 4 = the reference's active
+                           4<->2 blend; 6 = 6<->4 and 8 = 8<->6 blends (blend weights the higher
+                           order; the paper's pipes used 6 with blend 0.4); 10, 12, 14 = fixed
+                           sets (blend unused). Orders above 4 reach K*d1 cells (K = 3, 4, 5, 6,
+                           8) and run on the one-column kernel: FP32 with K*d1 <= 8, FP64 with
+                           K*d1 <= 4; FP16 storage supports orders 0/4 only. Not in param.txt. */
 } fslbm_params;
 
 /* One monitor record (FSLBM.cu:632-666): means over the first fluid plane (q1, p1) and over the
@@ -140,6 +146,9 @@ int fslbm_solve_device_fields(fslbm_solve* s, void** p, void** u, void** v, void
  * (no host arrays, no copies); asynchronous on the context's stream. modes <= 16. */
 int fslbm_solve_init_poiseuille(fslbm_solve* s, double umax, double noise, int modes,
                                 double mode_amp, uint64_t seed);
+/* Corrector coefficients c0..c8 of an order and blend as the solve of `dtype` uses them (FP32
+ * forms for FP32 and FP16 storage); *taps = K. FSLBM_ERR_ARG for an unknown order. */
+int fslbm_fd_coefficients(int order, double blend, fslbm_dtype dtype, double* c, int* taps);
 /* Device bytes fslbm_solve_create allocates for a domain and dtype (an upper bound). */
 int fslbm_solve_footprint(const fslbm_domain* dom, fslbm_dtype dtype, int64_t* bytes);
 

@@ -5,6 +5,7 @@
 // What it restates (file:line in PipeDemoStandalone/FSLBM.cu of alparmat/FlowContrast):
 //   predictor  (D3Q27 equilibrium pull, wall rule "p_n := p_centre")   FSLBM.cu:60-63, 130-173
 //   corrector  (coarse-stride FD reverse diffusion, order 2<->4 blend)   FSLBM.cu:231-257, 269-273
+//              and the orders 6..14 / blends the reference keeps as alternatives  FSLBM.cu:177-229
 //   constants  dtddy = nu - 0.16666666, m = 1/d1^2                       FSLBM.cu:599, 624
 //   boundaries walls := 0, buffer planes := copy +-pin, gauge p -= p2   FSLBM.cu:280-303
 //   step order sweep -> BC(gauge of step c-1) -> monitor every 50 steps FSLBM.cu:620-647
@@ -48,14 +49,54 @@ constexpr int BUF = 1;
 
 template <class T> struct Consts {
   T tb, cc, pin, dtddy, m, c0, c1, c2, gauge, fx, fy, fz;
-  int d1;
+  T c[9];   // c[0] = c0 .. c[K]: corrector coefficients
+  int d1, K;
 };
+
+// Corrector coefficient sets of FSLBM.cu:177-232 (orders 14..2 and the 8<->6, 6<->4, 4<->2
+// blends; only 4<->2 is active in the reference, the others are its commented alternatives),
+// formed in T as the reference forms its active set. order 0 or 4: the 4<->2 blend; 6: 6<->4;
+// 8: 8<->6 (blend weights the higher order); 10, 12, 14: fixed. Returns K (taps), 0 if unknown.
+template <class T>
+int fd_coefficients(int order, T b, T* c) {
+  for (int k = 0; k < 9; ++k) c[k] = T(0);
+  switch (order) {
+    case 0: case 4:
+      c[0] = T(-6.0) - T(1.5) * b; c[1] = T(1.0) + T(0.3333333333) * b; c[2] = T(-0.0833333333) * b;
+      return 2;
+    case 6:
+      c[0] = T(-7.5) - T(0.66666666666) * b; c[1] = T(1.3333333) + T(0.16666666666) * b;
+      c[2] = T(-0.08333333) - T(0.0666666666666) * b; c[3] = T(0.01111111) * b;
+      return 3;
+    case 8:
+      c[0] = T(-8.166666666666666) - T(0.375) * b; c[1] = T(1.5) + T(0.1) * b;
+      c[2] = T(-0.15) - T(0.05) * b; c[3] = T(0.01111111) + T(0.014285714285714) * b;
+      c[4] = T(-0.001785714285714) * b;
+      return 4;
+    case 10:
+      c[0] = T(-8.78166666666); c[1] = T(1.66666666); c[2] = T(-0.23809523809);
+      c[3] = T(0.03968253968); c[4] = T(-0.00496031746); c[5] = T(0.00031746031);
+      return 5;
+    case 12:
+      c[0] = T(-8.94833333333); c[1] = T(1.71428571429); c[2] = T(-0.26785714285);
+      c[3] = T(0.05291005291); c[4] = T(-0.00892857142); c[5] = T(0.00103896103);
+      c[6] = T(-0.00006012506);
+      return 6;
+    case 14:
+      c[0] = T(-9.16453231293); c[1] = T(1.77777777778); c[2] = T(-0.31111111111);
+      c[3] = T(0.07542087542); c[4] = T(-0.01767676767); c[5] = T(3.48096348e-3);
+      c[6] = T(-5.1800052e-4); c[7] = T(5.0742908e-5); c[8] = T(-2.4281274e-6);
+      return 8;
+    default:
+      return 0;
+  }
+}
 
 // Derive the per-step constants exactly as the reference forms them (FSLBM.cu:231, 269,
 // 599, 624). For T=float this reproduces the reference's float arithmetic on its inputs.
 template <class T>
 Consts<T> derive(const double* prm) {
-  // prm: tblend, pin, nu, d1, blend, gauge, fx, fy, fz
+  // prm: tblend, pin, nu, d1, blend, gauge, fx, fy, fz, fd_order
   Consts<T> k;
   k.tb = T(prm[0]);
   k.cc = T(1.0 - double(k.tb));                  // float cc=1.0-tblend (double then float)
@@ -65,9 +106,8 @@ Consts<T> derive(const double* prm) {
   k.d1 = int(prm[3]);
   k.m = T(1.0 / double(T(k.d1 * k.d1)));         // 1.0/float(d1*d1), FSLBM.cu:624
   const T blend = T(prm[4]);
-  k.c0 = T(-6.0) - T(1.5) * blend;               // FSLBM.cu:231
-  k.c1 = T(1.0) + T(0.3333333333) * blend;
-  k.c2 = T(-0.0833333333) * blend;
+  k.K = fd_coefficients<T>(int(prm[9]), blend, k.c);   // FSLBM.cu:231 for orders 0/4
+  k.c0 = k.c[0]; k.c1 = k.c[1]; k.c2 = k.c[2];
   k.gauge = T(prm[5]);
   k.fx = T(prm[6]); k.fy = T(prm[7]); k.fz = T(prm[8]);
   return k;
@@ -147,17 +187,17 @@ void step_ref(const uint8_t* io, int lx, int ly, int lz, int d2, const Consts<T>
           uy2 += K.c1 * (b0 + b1 + b2 + b3 + b4 + b5);
           uz2 += K.c1 * (e0 + e1 + e2 + e3 + e4 + e5);
         }
-        {
-          const int o = 2 * d1;
+        for (int kk = 2; kk <= K.K; ++kk) {             // taps at 2*d1 .. K*d1
+          const int o = kk * d1;
           const T a0 = tex(iu, x + o, y, z), a1 = tex(iu, x - o, y, z), a2 = tex(iu, x, y + o, z),
                   a3 = tex(iu, x, y - o, z), a4 = tex(iu, x, y, z + o), a5 = tex(iu, x, y, z - o);
           const T b0 = tex(iv, x + o, y, z), b1 = tex(iv, x - o, y, z), b2 = tex(iv, x, y + o, z),
                   b3 = tex(iv, x, y - o, z), b4 = tex(iv, x, y, z + o), b5 = tex(iv, x, y, z - o);
           const T e0 = tex(iw, x + o, y, z), e1 = tex(iw, x - o, y, z), e2 = tex(iw, x, y + o, z),
                   e3 = tex(iw, x, y - o, z), e4 = tex(iw, x, y, z + o), e5 = tex(iw, x, y, z - o);
-          ux2 += K.c2 * (a0 + a1 + a2 + a3 + a4 + a5);
-          uy2 += K.c2 * (b0 + b1 + b2 + b3 + b4 + b5);
-          uz2 += K.c2 * (e0 + e1 + e2 + e3 + e4 + e5);
+          ux2 += K.c[kk] * (a0 + a1 + a2 + a3 + a4 + a5);
+          uy2 += K.c[kk] * (b0 + b1 + b2 + b3 + b4 + b5);
+          uz2 += K.c[kk] * (e0 + e1 + e2 + e3 + e4 + e5);
         }
         // FSLBM.cu:269-273 (+ optional body force, exact +0 when unused)
         sp[idx] = rt1;
@@ -256,9 +296,12 @@ void monitor_ref(const uint8_t* io, int lx, int ly, int lz, int d2, double nu, d
 template <class T>
 int run_core(const uint8_t* mask2d, int lx, int ly, int L, const double* prm, int monitor_every,
              double radius, long nsteps, T* fields, double* mon_out, int nthreads) {
-  // prm: tblend, pin, nu, d1, blend, fx, fy, fz (gauge is driven here)
+  // prm: tblend, pin, nu, d1, blend, fx, fy, fz, fd_order (gauge is driven here)
   const int d1 = int(prm[3]);
-  const int d2 = std::max(1, 2 * d1);
+  double cdum[9];
+  const int K = fd_coefficients<double>(int(prm[8]), 0.0, cdum);
+  if (K == 0) return -6;
+  const int d2 = std::max(1, K * d1);                         // buffers cover the corrector reach
   if (L < d2 + 1) return -5;
   for (int y = 0; y < ly; ++y)
     for (int x = 0; x < lx; ++x) {
@@ -273,8 +316,8 @@ int run_core(const uint8_t* mask2d, int lx, int ly, int L, const double* prm, in
   double gauge = 0.0;
   long nmon = 0;
   for (long c = 1; c <= nsteps; ++c) {
-    double p9[9] = {prm[0], prm[1], prm[2], prm[3], prm[4], gauge, prm[5], prm[6], prm[7]};
-    const Consts<T> K = derive<T>(p9);
+    double p10[10] = {prm[0], prm[1], prm[2], prm[3], prm[4], gauge, prm[5], prm[6], prm[7], prm[8]};
+    const Consts<T> K = derive<T>(p10);
     pad_core(mask2d, lx, ly, L, d2, K.pin, fields, io, a);
     step_ref<T>(io.data(), lx, ly, lz, d2, K, a.data(), b.data(), nthreads);
     gauge = 0.0;                                              // FSLBM.cu:628
@@ -300,7 +343,7 @@ int oracle_check_ref_mask(const uint8_t* io, int lx, int ly, int lz, int d2) {
   return check_ref_mask(io, lx, ly, lz, d2);
 }
 
-// One reference-layout step. prm: tblend, pin, nu, d1, blend, gauge(p2), fx, fy, fz.
+// One reference-layout step. prm: tblend, pin, nu, d1, blend, gauge(p2), fx, fy, fz, fd_order.
 // in/out: 4*lx*ly*lz values (p block, u block, v block, w block).
 int oracle_step_ref_f64(const uint8_t* io, int lx, int ly, int lz, int d2, const double* prm,
                         const double* in, double* out, int nthreads) {
@@ -330,8 +373,8 @@ int oracle_monitor_ref_f32(const uint8_t* io, int lx, int ly, int lz, int d2, do
 
 // Periodic-core run: cross-section mask (lx*ly, 0 fluid / 125 wall) extruded over L planes,
 // streamwise wrap with the +-pin pressure jump across the seam, realised by padding the core
-// with d2 = max(1, 2*d1) reference buffer planes each step. prm: tblend, pin, nu, d1, blend,
-// fx, fy, fz. Monitor every `monitor_every` steps (0: never); records (7 doubles each) go to
+// with d2 = max(1, K*d1) reference buffer planes each step (K corrector taps). prm: tblend, pin,
+// nu, d1, blend, fx, fy, fz, fd_order. Monitor every `monitor_every` steps (0: never); records (7 doubles each) go to
 // mon_out. Returns the number of monitor records or a negative code.
 int oracle_run_core_f64(const uint8_t* mask2d, int lx, int ly, int L, const double* prm,
                         int monitor_every, double radius, long nsteps, double* fields,
@@ -386,6 +429,11 @@ int oracle_pipe_m_mask(int lx0, int l0, int d, uint8_t* out) {
         out[(i - 1) + long(lx) * ((j - 1) + long(lx) * (k - 1))] = v;
       }
   return 0;
+}
+
+// Corrector coefficients c0..c8 (FP64 forms) of an order; returns the tap count K or 0.
+int oracle_fd_coefficients(int order, double blend, double* c) {
+  return fd_coefficients<double>(order, blend, c);
 }
 
 int oracle_max_threads(void) {

@@ -37,6 +37,7 @@ def lib():
         L.oracle_stats_accumulate.restype = None
         L.oracle_pipe_m_mask.argtypes = [i, i, i, _u8p]
         L.oracle_max_threads.argtypes = []
+        L.oracle_fd_coefficients.argtypes = [i, d, _f64p]
         _lib = L
     return _lib
 
@@ -58,7 +59,8 @@ def step_ref(io, fields, prm, dtype=np.float64, nthreads=0):
     lz, ly, lx = io.shape
     d2 = prm.get("d2", 10)
     p = np.array([prm["tblend"], prm["pin"], prm["nu"], prm["d1"], prm["blend"],
-                  prm.get("gauge", 0.0), *prm.get("force", (0.0, 0.0, 0.0))], np.float64)
+                  prm.get("gauge", 0.0), *prm.get("force", (0.0, 0.0, 0.0)),
+                  prm.get("fd_order", 0)], np.float64)
     src = np.ascontiguousarray(fields, dtype=dtype)
     out = np.empty_like(src)
     fn = lib().oracle_step_ref_f64 if dtype == np.float64 else lib().oracle_step_ref_f32
@@ -84,7 +86,7 @@ def run_core(mask2d, L, fields, prm, nsteps, monitor_every=50, radius=0.0, dtype
     """Periodic-core run. mask2d (ly,lx) 0/125; fields (4,L,ly,lx). Returns (fields, monitor)."""
     ly, lx = mask2d.shape
     p = np.array([prm["tblend"], prm["pin"], prm["nu"], prm["d1"], prm["blend"],
-                  *prm.get("force", (0.0, 0.0, 0.0))], np.float64)
+                  *prm.get("force", (0.0, 0.0, 0.0)), prm.get("fd_order", 0)], np.float64)
     f = np.array(fields, dtype=dtype, order="C", copy=True)
     nmon = nsteps // monitor_every if monitor_every > 0 else 0
     mon = np.zeros((max(nmon, 1), 7))
@@ -100,3 +102,12 @@ def stats_accumulate(acc, p, u, v, w, cnt):
     n = p.size
     lib().oracle_stats_accumulate(n, *(np.ascontiguousarray(a, np.float64).ravel() for a in (p, u, v, w)),
                                   int(cnt), acc.ravel())
+
+
+def fd_coefficients(order, blend=0.0):
+    """Corrector coefficients c0..cK of an order (the reference's sets), FP64 forms."""
+    c = np.zeros(9)
+    k = lib().oracle_fd_coefficients(int(order), float(blend), c)
+    if k == 0:
+        raise ValueError(f"no corrector of order {order}")
+    return c[:k + 1]

@@ -35,7 +35,7 @@ def config1(fb, L=64, lx=32, ly=32, R=15.0, Re=100.0, nu=0.01, noise=1e-3, seed=
 def to_params(fb, prm, monitor_every=50, delta=1):
     return fb.Params.make(tblend=prm["tblend"], pin=prm["pin"], nu=prm["nu"], d1=prm["d1"],
                           delta=delta, blend=prm["blend"], monitor_every=monitor_every,
-                          force=prm.get("force", (0.0, 0.0, 0.0)))
+                          force=prm.get("force", (0.0, 0.0, 0.0)), fd_order=prm.get("fd_order", 0))
 
 
 def run_gpu(fb, ctx, dom, prm, dtype, f, nsteps, monitor_every=50):
