@@ -35,7 +35,7 @@ class Domain(ctypes.Structure):
     _fields_ = [("lx", ctypes.c_int), ("ly", ctypes.c_int), ("lz", ctypes.c_int),
                 ("mask", ctypes.c_void_p), ("radius", ctypes.c_double),
                 ("cx", ctypes.c_double), ("cy", ctypes.c_double),
-                ("buffer_depth", ctypes.c_int)]
+                ("buffer_depth", ctypes.c_int), ("mask_planes", ctypes.c_int)]
 
 
 class Params(ctypes.Structure):
@@ -190,6 +190,7 @@ def lib():
             "fslbm_write_param_txt": ([ctypes.c_char_p, ctypes.POINTER(Params)], _i),
             "fslbm_pipe_m_mask": ([_i, _i, _i, _vp], _i),
             "fslbm_ref_mask_to_core": ([_vp, _i, _i, _i, _i, _vp], _i),
+            "fslbm_ref_mask_to_core3d": ([_vp, _i, _i, _i, _i, _vp], _i),
             "fslbm_init_poiseuille": ([ctypes.POINTER(Domain), ctypes.c_double, ctypes.c_double,
                                        _i, ctypes.c_double, ctypes.c_uint64, _vp, _vp, _vp, _vp], _i),
         }
@@ -254,13 +255,29 @@ def ref_mask_to_core(mask3d, d2=10):
     return out
 
 
+def ref_mask_to_core3d(mask3d, d2=10):
+    """Reference-layout mask (lz_ref, ly, lx) -> core masks (lz_ref - 2*d2, ly, lx), one
+    cross-section per core plane (buffers must copy the wrapped core planes)."""
+    mask3d = np.ascontiguousarray(mask3d, np.uint8)
+    lz, ly, lx = mask3d.shape
+    out = np.empty((lz - 2 * d2, ly, lx), np.uint8)
+    _check(lib().fslbm_ref_mask_to_core3d(_ptr(mask3d), lx, ly, lz, d2, _ptr(out)))
+    return out
+
+
 def make_domain(lx, ly, lz, mask=None, radius=0.0, cx=None, cy=None, buffer_depth=10):
-    """Domain struct; keeps a reference to the mask array on the struct."""
+    """Domain struct; keeps a reference to the mask array on the struct. mask: (ly, lx) for a
+    cross-section extruded along z, or (lz, ly, lx) for one cross-section per plane."""
     d = Domain(lx, ly, lz, None, float(radius),
                float((lx - 1) / 2 if cx is None else cx), float((ly - 1) / 2 if cy is None else cy),
-               int(buffer_depth))
+               int(buffer_depth), 0)
     if mask is not None:
-        m = np.ascontiguousarray(mask, np.uint8).reshape(ly, lx)
+        m = np.ascontiguousarray(mask, np.uint8)
+        if m.ndim == 3:
+            m = m.reshape(lz, ly, lx)
+            d.mask_planes = lz
+        else:
+            m = m.reshape(ly, lx)
         d.mask = m.ctypes.data
         d._mask_ref = m
     return d

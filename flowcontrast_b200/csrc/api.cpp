@@ -155,7 +155,10 @@ struct fslbm_solve {
   size_t es = 4;
   fslbm_params prm{};
   std::vector<uint8_t> mask;   // lxp*ly, padded columns are wall
-  int64_t fluid2d = 0;
+  int64_t fluid2d = 0;             // fluid cells of the (first) cross-section
+  double l1 = 0;                   // the monitor's l1 (FSLBM.cu:589-591)
+  int64_t fluid_total = 0;         // fluid cells of the core
+  int planes = 1;                  // mask cross-sections: 1 (extruded) or L (one per plane)
   int sx = 0, sy = 0, sz = 0;  // monitor sample cell
   // device
   void* state[2] = {nullptr, nullptr};
@@ -196,6 +199,11 @@ struct fslbm_solve {
 };
 
 static size_t field_stride(const fslbm_solve* s) { return size_t(s->lxp) * s->ly * s->L; }
+
+// Mask byte of cell (x, y) in core plane z (one cross-section, or one per plane).
+static uint8_t mask_at(const fslbm_solve* s, int x, int y, int z) {
+  return s->mask[((s->planes > 1 ? size_t(z) : 0) * s->ly + y) * s->lxp + x];
+}
 
 // Milliseconds between two events, if both were recorded. A failed query (events never
 // recorded) is cleared from the runtime's last-error slot, where a later launch check would
@@ -270,9 +278,10 @@ static std::vector<int2> fluid_tiles(const fslbm_solve* s, int th) {
   for (int y0 = 0; y0 < s->ly; y0 += th)
     for (int x0 = 0; x0 < s->lxp; x0 += kTX) {
       bool any = false;
-      for (int y = y0; y < std::min(y0 + th, s->ly) && !any; ++y)
-        for (int x = x0; x < std::min(x0 + kTX, s->lxp); ++x)
-          if (s->mask[size_t(y) * s->lxp + x] == 0) { any = true; break; }
+      for (int z = 0; z < s->planes && !any; ++z)
+        for (int y = y0; y < std::min(y0 + th, s->ly) && !any; ++y)
+          for (int x = x0; x < std::min(x0 + kTX, s->lxp); ++x)
+            if (s->mask[(size_t(z) * s->ly + y) * s->lxp + x] == 0) { any = true; break; }
       if (any) tiles.push_back(make_int2(x0, y0));
     }
   return tiles;
@@ -289,7 +298,7 @@ static int configure_kernel(fslbm_solve* s) {
   double cf[9];
   s->K = fd_coefficients(s->prm.fd_order, s->prm.blend, s->dtype != FSLBM_F64, cf);
   // FP16 storage exists only in the column-pair kernel, which has the 2-tap corrector
-  s->use2 = step2_supported(s->dtype, s->prm.d1) && s->K == 2 &&
+  s->use2 = step2_supported(s->dtype, s->prm.d1) && s->K == 2 && s->planes == 1 &&
             (s->dtype == FSLBM_F16 || !(ek && std::atoi(ek) == 1));
   s->ty2 = (et && std::atoi(et) == 16) ? 16 : 32;
   const char* ep = std::getenv("FSLBM_PACKED");
@@ -358,6 +367,35 @@ static std::vector<ColCoef<TC>> column_coefs(const fslbm_solve* s) {
       c.ws0 = TC(a); c.wsx = TC(bx); c.wsy = TC(by);
       c.fluid = TC(s->mask[size_t(y) * s->lxp + x] == 0 ? 1 : 0);
     }
+  return cc;
+}
+
+// Wall sums per cell for masks that vary along z: sums of w(cx)w(cy)w(cz) c^k over the wall
+// cells of the 3x3x3 neighbourhood (periodic in z, outside the cross-section counts as wall).
+template <class TC>
+static std::vector<CellCoef<TC>> cell_coefs(const fslbm_solve* s) {
+  const size_t plane = size_t(s->lxp) * s->ly;
+  std::vector<CellCoef<TC>> cc(plane * s->L);
+  const double wv[3] = {1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0};
+  for (int z = 0; z < s->L; ++z)
+    for (int y = 0; y < s->ly; ++y)
+      for (int x = 0; x < s->lxp; ++x) {
+        double a = 0, bx = 0, by = 0, bz = 0;
+        for (int dz = -1; dz <= 1; ++dz) {
+          const int gz = (z + dz + s->L) % s->L;
+          for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+              const int gx = x + dx, gy = y + dy;
+              const bool wall = gx < 0 || gy < 0 || gx >= s->lxp || gy >= s->ly ||
+                                s->mask[gz * plane + size_t(gy) * s->lxp + gx] == kWall;
+              if (!wall) continue;
+              const double w = wv[dx + 1] * wv[dy + 1] * wv[dz + 1];
+              a += w; bx += dx * w; by += dy * w; bz += dz * w;
+            }
+        }
+        CellCoef<TC>& c = cc[z * plane + size_t(y) * s->lxp + x];
+        c.ws0 = TC(a); c.wsx = TC(bx); c.wsy = TC(by); c.wsz = TC(bz);
+      }
   return cc;
 }
 
@@ -430,38 +468,60 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
   s->dtype = dtype;
   s->es = dtype == FSLBM_F64 ? 8 : (dtype == FSLBM_F16 ? 2 : 4);
   s->prm = *prm;
-  s->mask.assign(size_t(s->lxp) * s->ly, kWall);
+  if (dom->mask_planes > 1 && (dom->mask_planes != dom->lz || !dom->mask)) {
+    free_solve(s);
+    return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: mask_planes must be 0, 1 or lz (%d) with a mask", dom->lz);
+  }
+  s->planes = dom->mask_planes > 1 ? dom->lz : 1;
+  const size_t plane = size_t(s->lxp) * s->ly;
+  s->mask.assign(plane * s->planes, kWall);
+  std::vector<int64_t> per_plane(s->planes, 0);
   double sxs = 0, sys = 0;
-  for (int y = 0; y < s->ly; ++y)
-    for (int x = 0; x < s->lx; ++x) {
-      uint8_t v;
-      if (dom->mask) {
-        v = dom->mask[size_t(y) * s->lx + x];
-        if (v != 0 && v != kWall) {
-          free_solve(s);
-          return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: mask value %d at (%d,%d); expected 0 or 125", v, x, y);
+  for (int z = 0; z < s->planes; ++z)
+    for (int y = 0; y < s->ly; ++y)
+      for (int x = 0; x < s->lx; ++x) {
+        uint8_t v;
+        if (dom->mask) {
+          v = dom->mask[(size_t(z) * s->ly + y) * s->lx + x];
+          if (v != 0 && v != kWall) {
+            free_solve(s);
+            return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: mask value %d at (%d,%d,%d); expected 0 or 125",
+                                   v, x, y, z);
+          }
+        } else {
+          const double dx = x - dom->cx, dy = y - dom->cy;
+          v = (dx * dx + dy * dy <= dom->radius * dom->radius) ? 0 : kWall;
         }
-      } else {
-        const double dx = x - dom->cx, dy = y - dom->cy;
-        v = (dx * dx + dy * dy <= dom->radius * dom->radius) ? 0 : kWall;
+        if (v == 0 && (x == 0 || y == 0 || x == s->lx - 1 || y == s->ly - 1)) {
+          free_solve(s);
+          return fslbm_set_error(FSLBM_ERR_ARG,
+                                 "solve_create: fluid cell (%d,%d,%d) on the box rim; the cross-section must "
+                                 "be enclosed by wall", x, y, z);
+        }
+        s->mask[z * plane + size_t(y) * s->lxp + x] = v;
+        if (v == 0) { ++per_plane[z]; sxs += x; sys += y; }
       }
-      if (v == 0 && (x == 0 || y == 0 || x == s->lx - 1 || y == s->ly - 1)) {
-        free_solve(s);
-        return fslbm_set_error(FSLBM_ERR_ARG,
-                               "solve_create: fluid cell (%d,%d) on the box rim; the cross-section must be "
-                               "enclosed by wall", x, y);
-      }
-      s->mask[size_t(y) * s->lxp + x] = v;
-      if (v == 0) { ++s->fluid2d; sxs += x; sys += y; }
-    }
-  if (s->fluid2d == 0) {
+  for (int64_t c : per_plane) s->fluid_total += c;
+  if (s->planes == 1) s->fluid_total *= s->L;
+  if (s->fluid_total == 0) {
     free_solve(s);
     return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: no fluid cells");
   }
+  // l1 of the monitor: the reference counts its buffer cells over 2*d2 planes (FSLBM.cu:589-591),
+  // i.e. the mean fluid count of the core planes the buffers copy
+  {
+    const int d2 = std::max(1, std::min(s->d2 > 0 ? s->d2 : 1, s->L));
+    int64_t c = 0;
+    for (int j = 0; j < d2; ++j) c += per_plane[s->planes == 1 ? 0 : j] + per_plane[s->planes == 1 ? 0 : s->L - 1 - j];
+    s->l1 = double(c) / double(2 * d2);
+    if (s->l1 <= 0) s->l1 = 1.0;
+    s->fluid2d = per_plane[0];
+  }
+  const double nfl = s->planes == 1 ? double(per_plane[0]) : double(s->fluid_total);
   s->from_mask = dom->mask != nullptr;
-  s->radius = dom->radius > 0 ? dom->radius : std::sqrt(double(s->fluid2d) / M_PI);
-  s->cx = dom->mask ? sxs / s->fluid2d : dom->cx;
-  s->cy = dom->mask ? sys / s->fluid2d : dom->cy;
+  s->radius = dom->radius > 0 ? dom->radius : std::sqrt(double(s->fluid_total) / s->L / M_PI);
+  s->cx = dom->mask ? sxs / nfl : dom->cx;
+  s->cy = dom->mask ? sys / nfl : dom->cy;
   // monitor sample: linear index (ly*lx)/2 + lx/2 of the plane z = lz_ref/2 (FSLBM.cu:653,665)
   {
     const long idx = (long(s->ly) * s->lx) / 2 + s->lx / 2;
@@ -487,7 +547,23 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
   if ((e = dalloc(s, &s->d_mask, s->mask.size()))) return fail("mask");
   if ((e = cudaMemcpyAsync(s->d_mask, s->mask.data(), s->mask.size(), cudaMemcpyHostToDevice, st)))
     return fail("mask copy");
-  if (dtype == FSLBM_F64) {
+  if (s->planes > 1 && dtype == FSLBM_F16) {
+    e = cudaErrorInvalidValue;
+    const int r = fslbm_set_error(FSLBM_ERR_ARG, "solve_create: masks varying along z need FP32 or FP64 storage");
+    free_solve(s);
+    return r;
+  }
+  if (s->planes > 1 && dtype == FSLBM_F64) {
+    auto cc = cell_coefs<double>(s);
+    if ((e = dalloc(s, &s->d_colcoef, cc.size() * sizeof(cc[0])))) return fail("colcoef");
+    e = cudaMemcpyAsync(s->d_colcoef, cc.data(), cc.size() * sizeof(cc[0]), cudaMemcpyHostToDevice, st);
+    if (!e) e = cudaStreamSynchronize(st);       // the table is a local vector
+  } else if (s->planes > 1) {
+    auto cc = cell_coefs<float>(s);
+    if ((e = dalloc(s, &s->d_colcoef, cc.size() * sizeof(cc[0])))) return fail("colcoef");
+    e = cudaMemcpyAsync(s->d_colcoef, cc.data(), cc.size() * sizeof(cc[0]), cudaMemcpyHostToDevice, st);
+    if (!e) e = cudaStreamSynchronize(st);
+  } else if (dtype == FSLBM_F64) {
     auto cc = column_coefs<double>(s);
     if ((e = dalloc(s, &s->d_colcoef, cc.size() * sizeof(cc[0])))) return fail("colcoef");
     e = cudaMemcpyAsync(s->d_colcoef, cc.data(), cc.size() * sizeof(cc[0]), cudaMemcpyHostToDevice, st);
@@ -569,9 +645,9 @@ extern "C" int fslbm_solve_set_fields(fslbm_solve* s, fslbm_dtype hd, const void
     CUDA_TRY(launch_convert_in(s->dtype, dst, s->d_stage, hd == FSLBM_F64, s->lx, s->lxp, s->ly,
                                s->L, st));
   }
-  CUDA_TRY(launch_zero_walls(s->dtype, dst, s->d_mask, s->lxp, s->ly, s->L, st));
+  CUDA_TRY(launch_zero_walls(s->dtype, dst, s->d_mask, s->planes, s->lxp, s->ly, s->L, st));
   // the other buffer's walls (never written by the step) must be zero too
-  CUDA_TRY(launch_zero_walls(s->dtype, s->state[1 - s->cur], s->d_mask, s->lxp, s->ly, s->L, st));
+  CUDA_TRY(launch_zero_walls(s->dtype, s->state[1 - s->cur], s->d_mask, s->planes, s->lxp, s->ly, s->L, st));
   s->fields_set = true;
   return FSLBM_OK;
 }
@@ -598,8 +674,8 @@ extern "C" int fslbm_solve_init_poiseuille(fslbm_solve* s, double umax, double n
   if (int r = fslbm_poiseuille_setup(&dom, umax, noise, modes, mode_amp, seed, &q, &fluid)) return r;
   CUDA_TRY(cudaSetDevice(s->ctx->device));
   cudaStream_t st = s->ctx->stream;
-  CUDA_TRY(launch_init_poiseuille(s->dtype, s->state[s->cur], s->d_mask, s->lxp, q, st));
-  CUDA_TRY(launch_zero_walls(s->dtype, s->state[1 - s->cur], s->d_mask, s->lxp, s->ly, s->L, st));
+  CUDA_TRY(launch_init_poiseuille(s->dtype, s->state[s->cur], s->d_mask, s->planes, s->lxp, q, st));
+  CUDA_TRY(launch_zero_walls(s->dtype, s->state[1 - s->cur], s->d_mask, s->planes, s->lxp, s->ly, s->L, st));
   s->fields_set = true;
   return FSLBM_OK;
 }
@@ -614,7 +690,11 @@ extern "C" int fslbm_solve_footprint(const fslbm_domain* dom, fslbm_dtype dtype,
   const int64_t lxp = (dom->lx + 7) / 8 * 8, cs = lxp * dom->ly, fs = cs * dom->lz;
   const int64_t cc = dtype == FSLBM_F64 ? int64_t(sizeof(ColCoef<double>)) : int64_t(sizeof(ColCoef<float>));
   const int64_t tiles = ((lxp + kTX - 1) / kTX) * ((dom->ly + kTY - 1) / kTY) * int64_t(sizeof(int2));
-  *bytes = 2 * 4 * fs * es + cs + cs * cc + tiles + int64_t(sizeof(DevCounters)) +
+  const int64_t masks = dom->mask_planes > 1
+                            ? cs * dom->lz * (1 + int64_t(dtype == FSLBM_F64 ? sizeof(CellCoef<double>)
+                                                                                : sizeof(CellCoef<float>)))
+                            : cs + cs * cc;
+  *bytes = 2 * 4 * fs * es + masks + tiles + int64_t(sizeof(DevCounters)) +
            4096 * int64_t(sizeof(fslbm_monitor)) + int64_t(sizeof(double)) * 9 + int64_t(sizeof(unsigned));
   return FSLBM_OK;
 }
@@ -682,13 +762,13 @@ static int enqueue_steps(fslbm_solve* s, int64_t nsteps) {
   a.lxp = s->lxp; a.ly = s->ly; a.L = s->L;
   a.ntiles = s->ntiles; a.chunk = s->chunk; a.nchunks = s->nchunks;
   a.tiles = s->d_tiles; a.mask = s->d_mask; a.colcoef = s->d_colcoef;
-  a.err = s->d_err; a.counters = s->d_counters;
+  a.err = s->d_err; a.counters = s->d_counters; a.mask_planes = s->planes;
   fill_constants(s, a);
   MonitorLaunch m{};
   m.dtype = s->dtype; m.mask = s->d_mask;
   m.lxp = s->lxp; m.lx = s->lx; m.ly = s->ly; m.L = s->L;
   m.pin = s->dtype != FSLBM_F64 ? double(float(s->prm.pin)) : s->prm.pin;
-  m.nu = s->prm.nu; m.radius = s->radius; m.l1 = double(s->fluid2d);
+  m.nu = s->prm.nu; m.radius = s->radius; m.l1 = s->l1;
   m.sx = s->sx; m.sy = s->sy; m.sz = s->sz;
   m.log = s->d_log; m.log_cap = s->log_cap; m.gauge_out = s->d_gauge; m.counters = s->d_counters;
   const int me = s->prm.monitor_every;
@@ -795,7 +875,7 @@ extern "C" int fslbm_solve_check(fslbm_solve* s, double* max_abs_u) {
 extern "C" int fslbm_solve_info(fslbm_solve* s, fslbm_info* out) {
   if (!s || !out) return fslbm_set_error(FSLBM_ERR_ARG, "info: null argument");
   out->cells = int64_t(s->lx) * s->ly * s->L;
-  out->fluid_cells = s->fluid2d * s->L;
+  out->fluid_cells = s->fluid_total;
   out->bytes_device = s->bytes_device;
   out->steps = s->steps;
   out->lx_pitch = s->lxp;
@@ -859,7 +939,7 @@ extern "C" int fslbm_solve_get_fields_ref(fslbm_solve* s, float* p, float* u, fl
     if (jump)
       for (size_t j = 0; j < plane; ++j) {
         const int x = int(j % s->lx), y = int(j / s->lx);
-        if (s->mask[size_t(y) * s->lxp + x] == kWall) continue;
+        if (mask_at(s, x, y, zc) == kWall) continue;
         float& pv = p[plane * zr + j];
         pv = jump > 0 ? pv + pin : pv - pin;
       }
@@ -900,7 +980,7 @@ extern "C" int fslbm_solve_get_plane(fslbm_solve* s, int kind, int comp, float* 
       if (zc < 0) { zc += s->L; jump = 1; } else if (zc >= s->L) { zc -= s->L; jump = -1; }
       for (int y = 0; y < s->ly; ++y) {
         float val = buf[comp * n + size_t(zc) * s->ly + y];
-        if (comp == 0 && jump && s->mask[size_t(y) * s->lxp + xs] != kWall)
+        if (comp == 0 && jump && mask_at(s, xs, y, zc) != kWall)
           val = jump > 0 ? val + pin : val - pin;
         out[size_t(zr) * s->ly + y] = val;
       }
@@ -919,7 +999,7 @@ extern "C" int fslbm_solve_get_plane(fslbm_solve* s, int kind, int comp, float* 
     for (size_t j = 0; j < n; ++j) {
       float val = buf[comp * n + j];
       const int x = int(j % s->lx), y = int(j / s->lx);
-      if (comp == 0 && jump && s->mask[size_t(y) * s->lxp + x] != kWall)
+      if (comp == 0 && jump && mask_at(s, x, y, zc) != kWall)
         val = jump > 0 ? val + pin : val - pin;
       out[j] = val;
     }
@@ -954,7 +1034,7 @@ extern "C" int fslbm_stats_sample(fslbm_solve* s) {
   }
   s->cnt += 1; s->cnt2 += 1;                                   // FSLBM.cu:715
   const double pin = s->dtype != FSLBM_F64 ? double(float(s->prm.pin)) : s->prm.pin;
-  CUDA_TRY(launch_plane_stats(s->dtype, s->state[s->cur], s->d_mask, s->lxp, s->ly, s->L, s->d2,
+  CUDA_TRY(launch_plane_stats(s->dtype, s->state[s->cur], s->d_mask, s->planes, s->lxp, s->ly, s->L, s->d2,
                               s->lx / 2, pin, s->cnt, 1, 1, s->d_stats, st));
   return FSLBM_OK;
 }
@@ -1128,7 +1208,7 @@ static int batch_upload(fslbm_batch* b) {
     m.mon.dtype = s->dtype; m.mon.mask = s->d_mask;
     m.mon.lxp = s->lxp; m.mon.lx = s->lx; m.mon.ly = s->ly; m.mon.L = s->L;
     m.mon.pin = double(float(s->prm.pin)); m.mon.nu = s->prm.nu; m.mon.radius = s->radius;
-    m.mon.l1 = double(s->fluid2d); m.mon.sx = s->sx; m.mon.sy = s->sy; m.mon.sz = s->sz;
+    m.mon.l1 = s->l1; m.mon.sx = s->sx; m.mon.sy = s->sy; m.mon.sz = s->sz;
     m.mon.log = s->d_log; m.mon.log_cap = s->log_cap; m.mon.gauge_out = s->d_gauge;
     m.mon.counters = s->d_counters;
     m.state[0] = s->state[0]; m.state[1] = s->state[1];

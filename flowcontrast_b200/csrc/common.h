@@ -14,4 +14,10 @@ template <class TC> struct ColCoef {
   TC ws0, wsx, wsy, fluid;
 };
 
+// Per cell, for masks that vary along z: wall sums of the predictor over the 3x3x3
+// neighbourhood, including the streamwise moment (zero for extruded masks).
+template <class TC> struct CellCoef {
+  TC ws0, wsx, wsy, wsz;
+};
+
 }  // namespace fslbm

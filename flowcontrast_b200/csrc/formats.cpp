@@ -185,6 +185,40 @@ extern "C" int fslbm_ref_mask_to_core(const uint8_t* m, int lx, int ly, int lz_r
   return FSLBM_OK;
 }
 
+extern "C" int fslbm_ref_mask_to_core3d(const uint8_t* m, int lx, int ly, int lz_ref, int d2,
+                                        uint8_t* core) {
+  if (!m || !core || lx < 3 || ly < 3 || d2 < 1 || lz_ref <= 2 * d2)
+    return fslbm_set_error(FSLBM_ERR_ARG, "ref_mask_to_core3d: bad argument");
+  const size_t plane = size_t(lx) * ly;
+  const int L = lz_ref - 2 * d2;
+  if (L < d2)
+    return fslbm_set_error(FSLBM_ERR_ARG, "ref_mask_to_core3d: %d fluid planes shorter than the buffer depth %d", L, d2);
+  for (int zc = 0; zc < L; ++zc)
+    for (size_t j = 0; j < plane; ++j) {
+      const uint8_t v = m[plane * (zc + d2) + j];
+      if (v != 0 && v != kWall)
+        return fslbm_set_error(FSLBM_ERR_ARG, "ref_mask_to_core3d: value %d in fluid plane %d", int(v), zc + d2);
+      const int x = int(j % lx), y = int(j / lx);
+      if (v == 0 && (x == 0 || y == 0 || x == lx - 1 || y == ly - 1))
+        return fslbm_set_error(FSLBM_ERR_ARG, "ref_mask_to_core3d: fluid cell (%d,%d,%d) on the box rim", x, y,
+                               zc + d2);
+      core[plane * zc + j] = v;
+    }
+  // buffer planes must be the wrapped core planes (fluid marked 1), as bcond copies them
+  for (int z = 0; z < lz_ref; ++z) {
+    if (z >= d2 && z < lz_ref - d2) continue;
+    const int zc = z < d2 ? z - d2 + L : z - d2 - L;
+    for (size_t j = 0; j < plane; ++j) {
+      const uint8_t want = core[plane * zc + j] == kWall ? kWall : kBuf;
+      if (m[plane * z + j] != want)
+        return fslbm_set_error(FSLBM_ERR_ARG,
+                               "ref_mask_to_core3d: buffer plane %d cell %zu is %d, expected %d (a copy of "
+                               "core plane %d)", z, j, int(m[plane * z + j]), int(want), zc);
+    }
+  }
+  return FSLBM_OK;
+}
+
 // Geometry of the seeded start (shared by the host and device generators): fluid cells from the
 // mask or the circle; for a mask (or no radius) the centre is the fluid centroid and R the
 // largest centre distance plus half a cell.

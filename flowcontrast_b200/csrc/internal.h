@@ -32,6 +32,7 @@ struct StepLaunch {
   DevCounters* counters;     // steps incremented by the launch
   long long step_no;         // the time step this launch computes (1-based; rounding seed)
   int K;                     // corrector taps (2: the reference's order 2<->4 blend)
+  int mask_planes;           // 0/1: extruded cross-section; L: a mask (and CellCoef) per plane
   // constants in double; converted to the compute type by the launcher
   double tb, cc, pin, dtddy, m, c0, c1, c2, fx, fy, fz;
   double ch[6];              // corrector coefficients c3..c8
@@ -95,11 +96,12 @@ cudaError_t launch_batch_monitor(const BatchMon* mons, int n, int parity_after, 
                                  cudaStream_t st);
 
 // Seeded Poiseuille start written into a pitched state (walls and pad columns zero).
-cudaError_t launch_init_poiseuille(int dtype, void* state, const uint8_t* mask, int lxp,
+cudaError_t launch_init_poiseuille(int dtype, void* state, const uint8_t* mask, int planes, int lxp,
                                    const PoiseuilleInit& q, cudaStream_t st);
-cudaError_t launch_zero_walls(int dtype, void* state, const uint8_t* mask, int lxp, int ly, int L,
-                              cudaStream_t st);
-cudaError_t launch_plane_stats(int dtype, const void* state, const uint8_t* mask, int lxp, int ly,
+// masks: `planes` cross-sections of lxp*ly bytes (1: extruded along z)
+cudaError_t launch_zero_walls(int dtype, void* state, const uint8_t* mask, int planes, int lxp,
+                              int ly, int L, cudaStream_t st);
+cudaError_t launch_plane_stats(int dtype, const void* state, const uint8_t* mask, int planes, int lxp, int ly,
                                int L, int d2, int xs, double pin, int cnt, int do_mean,
                                int do_fluct, double* acc, cudaStream_t st);
 cudaError_t launch_profile(int dtype, const void* state, int lxp, int ly, int L, double* acc,

@@ -28,6 +28,7 @@ static cudaError_t launch_step_t(const StepLaunch& a, cudaStream_t st) {
   g.tiles = a.tiles; g.mask = a.mask; g.colcoef = a.colcoef; g.out = a.out;
   g.gauge = a.gauge; g.err = a.err;
   g.step_counter = a.counters ? &a.counters->steps : nullptr;
+  g.mask_planes = a.mask_planes;
   StepConst<TC> k;
   k.tb = TC(a.tb); k.cc = TC(a.cc); k.pin = TC(a.pin); k.dtddy = TC(a.dtddy); k.m = TC(a.m);
   k.c0 = TC(a.c0); k.c1 = TC(a.c1); k.c2 = TC(a.c2);
@@ -334,7 +335,8 @@ cudaError_t launch_monitor(const MonitorLaunch& a, cudaStream_t st) {
 // seeded initial fields generated on the device (same formula as the host generator)
 // ------------------------------------------------------------------------------------------
 template <class TS>
-__global__ void init_poiseuille_kernel(TS* s, const uint8_t* mask, int lxp, PoiseuilleInit q) {
+__global__ void init_poiseuille_kernel(TS* s, const uint8_t* mask, int planes, int lxp,
+                                       PoiseuilleInit q) {
   const size_t FS = size_t(lxp) * q.ly * q.L;
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < FS;
        i += size_t(gridDim.x) * blockDim.x) {
@@ -342,20 +344,21 @@ __global__ void init_poiseuille_kernel(TS* s, const uint8_t* mask, int lxp, Pois
     const size_t r = i / lxp;
     const int y = int(r % q.ly), z = int(r / q.ly);
     double c[4] = {0.0, 0.0, 0.0, 0.0};
-    if (x < q.lx && mask[size_t(y) * lxp + x] != kWall) poiseuille_cell(q, x, y, z, c);
+    if (x < q.lx && mask[(planes > 1 ? size_t(z) * q.ly : 0) * lxp + size_t(y) * lxp + x] != kWall)
+      poiseuille_cell(q, x, y, z, c);
     s[i] = TS(c[0]); s[FS + i] = TS(c[1]); s[2 * FS + i] = TS(c[2]); s[3 * FS + i] = TS(c[3]);
   }
 }
 
-cudaError_t launch_init_poiseuille(int dtype, void* state, const uint8_t* mask, int lxp,
+cudaError_t launch_init_poiseuille(int dtype, void* state, const uint8_t* mask, int planes, int lxp,
                                    const PoiseuilleInit& q, cudaStream_t st) {
   const int grid = 1184;
   if (dtype == FSLBM_F32)
-    init_poiseuille_kernel<float><<<grid, 256, 0, st>>>((float*)state, mask, lxp, q);
+    init_poiseuille_kernel<float><<<grid, 256, 0, st>>>((float*)state, mask, planes, lxp, q);
   else if (dtype == FSLBM_F64)
-    init_poiseuille_kernel<double><<<grid, 256, 0, st>>>((double*)state, mask, lxp, q);
+    init_poiseuille_kernel<double><<<grid, 256, 0, st>>>((double*)state, mask, planes, lxp, q);
   else if (dtype == FSLBM_F16)
-    init_poiseuille_kernel<__half><<<grid, 256, 0, st>>>((__half*)state, mask, lxp, q);
+    init_poiseuille_kernel<__half><<<grid, 256, 0, st>>>((__half*)state, mask, planes, lxp, q);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -364,25 +367,25 @@ cudaError_t launch_init_poiseuille(int dtype, void* state, const uint8_t* mask, 
 // wall zeroing, conversion, check
 // ------------------------------------------------------------------------------------------
 template <class TS>
-__global__ void zero_walls_kernel(TS* s, const uint8_t* mask, int lxp, int ly, int L) {
-  const size_t FS = size_t(lxp) * ly * L;
+__global__ void zero_walls_kernel(TS* s, const uint8_t* mask, int planes, int lxp, int ly, int L) {
+  const size_t FS = size_t(lxp) * ly * L, plane = size_t(lxp) * ly;
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < FS;
        i += size_t(gridDim.x) * blockDim.x) {
-    if (mask[i % (size_t(lxp) * ly)] == kWall) {
+    if (mask[planes > 1 ? i : i % plane] == kWall) {
       s[i] = TS(0); s[FS + i] = TS(0); s[2 * FS + i] = TS(0); s[3 * FS + i] = TS(0);
     }
   }
 }
 
-cudaError_t launch_zero_walls(int dtype, void* state, const uint8_t* mask, int lxp, int ly, int L,
-                              cudaStream_t st) {
+cudaError_t launch_zero_walls(int dtype, void* state, const uint8_t* mask, int planes, int lxp,
+                              int ly, int L, cudaStream_t st) {
   const int grid = 592;
   if (dtype == FSLBM_F32)
-    zero_walls_kernel<float><<<grid, 256, 0, st>>>(reinterpret_cast<float*>(state), mask, lxp, ly, L);
+    zero_walls_kernel<float><<<grid, 256, 0, st>>>(reinterpret_cast<float*>(state), mask, planes, lxp, ly, L);
   else if (dtype == FSLBM_F64)
-    zero_walls_kernel<double><<<grid, 256, 0, st>>>(reinterpret_cast<double*>(state), mask, lxp, ly, L);
+    zero_walls_kernel<double><<<grid, 256, 0, st>>>(reinterpret_cast<double*>(state), mask, planes, lxp, ly, L);
   else if (dtype == FSLBM_F16)
-    zero_walls_kernel<__half><<<grid, 256, 0, st>>>(reinterpret_cast<__half*>(state), mask, lxp, ly, L);
+    zero_walls_kernel<__half><<<grid, 256, 0, st>>>(reinterpret_cast<__half*>(state), mask, planes, lxp, ly, L);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -490,8 +493,8 @@ cudaError_t launch_check(int dtype, const void* state, size_t n_per_field, doubl
 // acc: 11 arrays of ly*(L+2*d2) doubles; cnt is the mean count including this sample.
 // ------------------------------------------------------------------------------------------
 template <class TS>
-__global__ void plane_stats_kernel(const TS* s, const uint8_t* mask, int lxp, int ly, int L,
-                                   int d2, int xs, double pin_d, int cnt, double* acc) {
+__global__ void plane_stats_kernel(const TS* s, const uint8_t* mask, int planes, int lxp, int ly,
+                                   int L, int d2, int xs, double pin_d, int cnt, double* acc) {
   const int Lr = L + 2 * d2;
   const size_t n = size_t(ly) * Lr, FS = size_t(lxp) * ly * L;
   using TA = typename ArithOf<TS>::type;
@@ -503,7 +506,7 @@ __global__ void plane_stats_kernel(const TS* s, const uint8_t* mask, int lxp, in
     if (zc < 0) { zc += L; jump = 1; } else if (zc >= L) { zc -= L; jump = -1; }
     const size_t o = (size_t(zc) * ly + y) * lxp + xs;
     TA p = TA(s[o]);
-    if (mask[size_t(y) * lxp + xs] != kWall) {
+    if (mask[(planes > 1 ? size_t(zc) * ly : 0) * lxp + size_t(y) * lxp + xs] != kWall) {
       if (jump == 1) p = TA(p + pin);
       else if (jump == -1) p = TA(p - pin);
     }
@@ -525,16 +528,16 @@ __global__ void plane_stats_kernel(const TS* s, const uint8_t* mask, int lxp, in
   }
 }
 
-cudaError_t launch_plane_stats(int dtype, const void* state, const uint8_t* mask, int lxp, int ly,
+cudaError_t launch_plane_stats(int dtype, const void* state, const uint8_t* mask, int planes, int lxp, int ly,
                                int L, int d2, int xs, double pin, int cnt, int, int, double* acc,
                                cudaStream_t st) {
   const int grid = 148;
   if (dtype == FSLBM_F32)
-    plane_stats_kernel<float><<<grid, 256, 0, st>>>((const float*)state, mask, lxp, ly, L, d2, xs, pin, cnt, acc);
+    plane_stats_kernel<float><<<grid, 256, 0, st>>>((const float*)state, mask, planes, lxp, ly, L, d2, xs, pin, cnt, acc);
   else if (dtype == FSLBM_F64)
-    plane_stats_kernel<double><<<grid, 256, 0, st>>>((const double*)state, mask, lxp, ly, L, d2, xs, pin, cnt, acc);
+    plane_stats_kernel<double><<<grid, 256, 0, st>>>((const double*)state, mask, planes, lxp, ly, L, d2, xs, pin, cnt, acc);
   else if (dtype == FSLBM_F16)
-    plane_stats_kernel<__half><<<grid, 256, 0, st>>>((const __half*)state, mask, lxp, ly, L, d2, xs, pin, cnt, acc);
+    plane_stats_kernel<__half><<<grid, 256, 0, st>>>((const __half*)state, mask, planes, lxp, ly, L, d2, xs, pin, cnt, acc);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }

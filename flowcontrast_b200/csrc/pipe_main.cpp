@@ -198,9 +198,15 @@ int main(int argc, char** argv) {
   std::vector<uint8_t> mask3d(cells_ref);
   if (fslbm_read_pipe_txt(path(o, "pipe.txt").c_str(), o.lx, o.ly, o.lz, mask3d.data()))
     return fail("pipe.txt");
+  // one cross-section extruded along the pipe if every plane has it, else one per plane
   std::vector<uint8_t> core(size_t(o.lx) * o.ly);
-  if (fslbm_ref_mask_to_core(mask3d.data(), o.lx, o.ly, o.lz, o.d2, core.data()))
-    return fail("pipe.txt geometry");
+  int mask_planes = 1;
+  if (fslbm_ref_mask_to_core(mask3d.data(), o.lx, o.ly, o.lz, o.d2, core.data())) {
+    core.assign(size_t(o.lx) * o.ly * L, 0);
+    if (fslbm_ref_mask_to_core3d(mask3d.data(), o.lx, o.ly, o.lz, o.d2, core.data()))
+      return fail("pipe.txt geometry");
+    mask_planes = L;
+  }
   const bool have_restart = exists(path(o, "p3Dii"));
   if (o.init == "restart" && !have_restart) {
     std::fprintf(stderr, "fslbm_pipe: --init restart but %s is missing\n", path(o, "p3Dii").c_str());
@@ -232,6 +238,7 @@ int main(int argc, char** argv) {
   fslbm_domain dom{};
   dom.lx = o.lx; dom.ly = o.ly; dom.lz = L; dom.mask = core.data(); dom.radius = o.radius;
   dom.buffer_depth = o.d2;
+  dom.mask_planes = mask_planes;
   fslbm_solve* s = nullptr;
   if (fslbm_solve_create(ctx, &dom, &prm, fslbm_dtype(o.dtype), &s)) return fail("solve");
   if (fslbm_solve_set_fields_ref(s, f[0].data(), f[1].data(), f[2].data(), f[3].data()))

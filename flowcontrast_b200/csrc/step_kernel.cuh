@@ -70,8 +70,9 @@ struct StepGeom {
   int lxp, ly, L;          // row pitch (padded lx), rows, streamwise planes
   int ntiles, chunk;       // tiles in the list; planes per chunk
   const int2* tiles;       // tile origins
-  const uint8_t* mask;     // lxp*ly: 0 fluid, 125 wall (padding columns are wall)
-  const void* colcoef;     // ColCoef<TC>[lxp*ly]
+  const uint8_t* mask;     // lxp*ly per plane: 0 fluid, 125 wall (padding columns are wall)
+  const void* colcoef;     // ColCoef<TC>[lxp*ly], or CellCoef<TC>[lxp*ly*L] for mask_planes > 1
+  int mask_planes;         // 0 or 1: one cross-section extruded along z; L: one per plane
   void* out;               // output state: 4 fields, field stride lxp*ly*L
   const double* gauge;     // p2 of the previous monitor (applied this step) or null
   unsigned* err;           // bit 0: a bounded wait gave up
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(TS) == 8 ? 1 : 2)
   }
   bool fluid = false;
   TC ws0 = 0, wsx = 0, wsy = 0;
-  if (x < g.lxp && y < g.ly) {
+  if (x < g.lxp && y < g.ly && g.mask_planes <= 1) {
     const ColCoef<TC> c = reinterpret_cast<const ColCoef<TC>*>(g.colcoef)[y * g.lxp + x];
     fluid = c.fluid != TC(0);
     ws0 = c.ws0; wsx = c.wsx; wsy = c.wsy;
@@ -159,11 +160,23 @@ __global__ void __launch_bounds__(kThreads, sizeof(TS) == 8 ? 1 : 2)
     const TS* pp = ring + size_t(pred ? (i - R + 1) % S : 0) * Tl::SLOT;
     if (pred) {
       const TC off = sp < 0 ? k.pin : (sp >= g.L ? -k.pin : TC(0));
+      // a mask per plane: the seam offset goes on the non-wall cells of the wrapped plane
+      const uint8_t* mz = nullptr;
+      if (g.mask_planes > 1 && off != TC(0)) {
+        int zz = sp % g.L;
+        if (zz < 0) zz += g.L;
+        mz = g.mask + size_t(zz) * g.lxp * g.ly;
+      }
       for (int j = tid; j < QN; j += kThreads) {
         const int e = (j / QW - 1 + HY) * SW + (j % QW - 1 + HX);
         const TC pv = TC(pp[e]), uv = TC(pp[PL + e]), vv = TC(pp[2 * PL + e]),
                  wv = TC(pp[3 * PL + e]);
-        q[j] = (nw[j] ? pv + off : pv) - TC(1.5) * (uv * uv + vv * vv + wv * wv);
+        bool nwj = nw[j];
+        if (mz) {
+          const int gx = org.x - 1 + j % QW, gy = org.y - 1 + j / QW;
+          nwj = gx >= 0 && gy >= 0 && gx < g.lxp && gy < g.ly && mz[gy * g.lxp + gx] != kWall;
+        }
+        q[j] = (nwj ? pv + off : pv) - TC(1.5) * (uv * uv + vv * vv + wv * wv);
       }
     }
     if (__syncthreads_or(!ok)) {
@@ -235,6 +248,13 @@ __global__ void __launch_bounds__(kThreads, sizeof(TS) == 8 ? 1 : 2)
     }
 
     const int zo = t - R;   // output plane; its predictor sums completed just above
+    TC wsz = 0;
+    if (g.mask_planes > 1 && zo >= zb && x < g.lxp && y < g.ly) {
+      const size_t cell = (size_t(zo) * g.ly + y) * g.lxp + x;
+      fluid = g.mask[cell] == 0;
+      const CellCoef<TC> c = reinterpret_cast<const CellCoef<TC>*>(g.colcoef)[cell];
+      ws0 = c.ws0; wsx = c.wsx; wsy = c.wsy; wsz = c.wsz;
+    }
     if (zo >= zb && fluid) {
       const TS* po = ring + size_t((i - R) % S) * Tl::SLOT + cidx;
       const TC pc = TC(po[0]);
@@ -254,12 +274,12 @@ __global__ void __launch_bounds__(kThreads, sizeof(TS) == 8 ? 1 : 2)
       const TC Lu = lap(po + PL, ru, uc), Lv = lap(po + 2 * PL, rv, vc),
                Lw = lap(po + 3 * PL, rw, wc);
       const TC rho = comp[0] + pc * ws0;
-      const TC us = comp[1] + pc * wsx, vs = comp[2] + pc * wsy, wsz = comp[3];
+      const TC us = comp[1] + pc * wsx, vs = comp[2] + pc * wsy, wzs = comp[3] + pc * wsz;
       const size_t o = (size_t(zo) * g.ly + y) * g.lxp + x;
       out[o] = TS(rho - gauge);
       out[FS + o] = TS((us + k.dtddy * Lu * k.m + k.fx) * k.tb + uc * k.cc);
       out[2 * FS + o] = TS((vs + k.dtddy * Lv * k.m + k.fy) * k.tb + vc * k.cc);
-      out[3 * FS + o] = TS((wsz + k.dtddy * Lw * k.m + k.fz) * k.tb + wc * k.cc);
+      out[3 * FS + o] = TS((wzs + k.dtddy * Lw * k.m + k.fz) * k.tb + wc * k.cc);
     }
   }
 }

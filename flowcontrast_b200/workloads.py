@@ -96,3 +96,26 @@ def request_stream(count, rate=200.0, seed=20261204, mixed_fraction=0.5):
         out.append(PipeSpec(L=L, n=n, re=re, seed=seed * 1000 + i, steps=steps, dtype=dtype,
                             arrival=t))
     return out
+
+
+def rough_pipe_mask(n, L, radius, amplitude=1.5, modes=3, seed=1):
+    """Seeded rough pipe (masks varying along z, one cross-section per plane), shape (L, n, n),
+    0 fluid / 125 wall: a cell is fluid where its distance from the axis is below
+    R(theta, z) = radius + amplitude * mean of `modes` sinusoids in theta (orders 3..) and z
+    (periodic over L, wavenumbers 1..), with seeded phases. The box rim stays wall."""
+    rng = np.random.default_rng(seed)
+    c = (n - 1) / 2.0
+    y, x = np.mgrid[0:n, 0:n]
+    r = np.hypot(x - c, y - c)
+    th = np.arctan2(y - c, x - c)
+    out = np.empty((L, n, n), np.uint8)
+    ph = rng.uniform(0, 2 * np.pi, size=(modes, 2))
+    for z in range(L):
+        bump = np.zeros_like(r)
+        for m in range(modes):
+            bump += np.sin((3 + m) * th + ph[m, 0]) * np.cos(2 * np.pi * (1 + m) * z / L + ph[m, 1])
+        rw = radius + amplitude * bump / modes
+        fluid = r <= rw
+        fluid[0, :] = fluid[-1, :] = fluid[:, 0] = fluid[:, -1] = False
+        out[z] = np.where(fluid, 0, 125)
+    return out

@@ -59,6 +59,12 @@ typedef struct {
   double radius;         /* circle radius; also the r of the friction factor and Re (FSLBM.cu:650,660) */
   double cx, cy;         /* circle centre: fluid iff (x-cx)^2 + (y-cy)^2 <= radius^2 */
   int buffer_depth;      /* d2 of the reference layout used by plane dumps and statistics */
+  int mask_planes;       /* 0 or 1: `mask` is one cross-section extruded along z; lz: `mask`
+                            holds lx*ly*lz values, one cross-section per plane (geometry that
+                            varies along the pipe, such as wall roughness; run on the one-column
+                            kernel, FP32/FP64). The monitor's l1, the reference's buffer-cell
+                            count over 2*d2 planes (FSLBM.cu:589-591), is then the mean fluid
+                            count of the buffer_depth planes at each end of the core. */
 } fslbm_domain;
 
 /* Run parameters: the six lines of param.txt (FSLBM.cu:502-507) plus additions. */
@@ -323,6 +329,11 @@ int fslbm_pipe_m_mask(int lx0, int l0, int d, uint8_t* out);
  * not the wrapped copies of their source planes. */
 int fslbm_ref_mask_to_core(const uint8_t* mask3d, int lx, int ly, int lz_ref, int d2,
                            uint8_t* mask2d_out);
+/* The same for geometry that varies along the pipe: core_out holds lx*ly*(lz_ref - 2*d2) values
+ * (one cross-section per core plane, for fslbm_domain.mask_planes = lz). Buffer planes must be
+ * the wrapped core planes, as the reference's bcond copies them (FSLBM.cu:291-301). */
+int fslbm_ref_mask_to_core3d(const uint8_t* mask3d, int lx, int ly, int lz_ref, int d2,
+                             uint8_t* core_out);
 /* Seeded initial fields (addition): Poiseuille w = -umax (1 - r^2/R^2) on the circle plus
  * uniform noise of amplitude noise*umax on u,v,w (splitmix64 of seed and cell index), and
  * `modes` random-phase sinusoidal streamwise/azimuthal perturbations of amplitude mode_amp*umax

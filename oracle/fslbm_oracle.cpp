@@ -245,10 +245,11 @@ int check_ref_mask(const uint8_t* io, int lx, int ly, int lz, int d2) {
 }
 
 template <class T>
-void pad_core(const uint8_t* mask2d, int lx, int ly, int L, int d2, T pin, const T* core,
+void pad_core(const uint8_t* mask, int planes, int lx, int ly, int L, int d2, T pin, const T* core,
               std::vector<uint8_t>& io, std::vector<T>& ref) {
   // Builds the reference layout (d2 buffer planes at each streamwise end, FSLBM.cu:291-301)
-  // from a periodic core whose cross-section mask is extruded along z.
+  // from a periodic core; mask holds one cross-section (planes = 1, extruded along z) or one
+  // per core plane (planes = L). Buffer planes carry the mask of the core plane they copy.
   const int lz = L + 2 * d2;
   const long nc = long(lx) * ly * L, nr = long(lx) * ly * lz, lxy = long(lx) * ly;
   io.assign(nr, 0);
@@ -257,9 +258,10 @@ void pad_core(const uint8_t* mask2d, int lx, int ly, int L, int d2, T pin, const
     int zc = z - d2; int jump = 0;
     if (zc < 0) { zc += L; jump = 1; }
     else if (zc >= L) { zc -= L; jump = -1; }
+    const uint8_t* mp = mask + (planes == 1 ? 0 : lxy * zc);
     for (long j = 0; j < lxy; ++j) {
       const long r = j + lxy * z, c = j + lxy * zc;
-      const bool wall = mask2d[j] == WALL;
+      const bool wall = mp[j] == WALL;
       io[r] = wall ? WALL : (jump ? BUF : 0);
       if (wall) continue;
       T pv = core[c];
@@ -294,8 +296,9 @@ void monitor_ref(const uint8_t* io, int lx, int ly, int lz, int d2, double nu, d
 }
 
 template <class T>
-int run_core(const uint8_t* mask2d, int lx, int ly, int L, const double* prm, int monitor_every,
-             double radius, long nsteps, T* fields, double* mon_out, int nthreads) {
+int run_core(const uint8_t* mask2d, int planes, int lx, int ly, int L, const double* prm,
+             int monitor_every, double radius, long nsteps, T* fields, double* mon_out,
+             int nthreads) {
   // prm: tblend, pin, nu, d1, blend, fx, fy, fz, fd_order (gauge is driven here)
   const int d1 = int(prm[3]);
   double cdum[9];
@@ -303,12 +306,14 @@ int run_core(const uint8_t* mask2d, int lx, int ly, int L, const double* prm, in
   if (K == 0) return -6;
   const int d2 = std::max(1, K * d1);                         // buffers cover the corrector reach
   if (L < d2 + 1) return -5;
-  for (int y = 0; y < ly; ++y)
-    for (int x = 0; x < lx; ++x) {
-      const uint8_t c = mask2d[x + long(lx) * y];
-      if (c != 0 && c != WALL) return -2;
-      if (c == 0 && (x == 0 || y == 0 || x == lx - 1 || y == ly - 1)) return -4;
-    }
+  if (planes != 1 && planes != L) return -1;
+  for (int z = 0; z < planes; ++z)
+    for (int y = 0; y < ly; ++y)
+      for (int x = 0; x < lx; ++x) {
+        const uint8_t c = mask2d[x + long(lx) * (y + long(ly) * z)];
+        if (c != 0 && c != WALL) return -2;
+        if (c == 0 && (x == 0 || y == 0 || x == lx - 1 || y == ly - 1)) return -4;
+      }
   const long nc = long(lx) * ly * L, lxy = long(lx) * ly;
   const int lz = L + 2 * d2;
   std::vector<uint8_t> io;
@@ -318,7 +323,7 @@ int run_core(const uint8_t* mask2d, int lx, int ly, int L, const double* prm, in
   for (long c = 1; c <= nsteps; ++c) {
     double p10[10] = {prm[0], prm[1], prm[2], prm[3], prm[4], gauge, prm[5], prm[6], prm[7], prm[8]};
     const Consts<T> K = derive<T>(p10);
-    pad_core(mask2d, lx, ly, L, d2, K.pin, fields, io, a);
+    pad_core(mask2d, planes, lx, ly, L, d2, K.pin, fields, io, a);
     step_ref<T>(io.data(), lx, ly, lz, d2, K, a.data(), b.data(), nthreads);
     gauge = 0.0;                                              // FSLBM.cu:628
     const long nr = long(lx) * ly * lz;
@@ -379,14 +384,29 @@ int oracle_monitor_ref_f32(const uint8_t* io, int lx, int ly, int lz, int d2, do
 int oracle_run_core_f64(const uint8_t* mask2d, int lx, int ly, int L, const double* prm,
                         int monitor_every, double radius, long nsteps, double* fields,
                         double* mon_out, int nthreads) {
-  return run_core<double>(mask2d, lx, ly, L, prm, monitor_every, radius, nsteps, fields, mon_out,
-                          nthreads);
+  return run_core<double>(mask2d, 1, lx, ly, L, prm, monitor_every, radius, nsteps, fields,
+                          mon_out, nthreads);
 }
 int oracle_run_core_f32(const uint8_t* mask2d, int lx, int ly, int L, const double* prm,
                         int monitor_every, double radius, long nsteps, float* fields,
                         double* mon_out, int nthreads) {
-  return run_core<float>(mask2d, lx, ly, L, prm, monitor_every, radius, nsteps, fields, mon_out,
-                         nthreads);
+  return run_core<float>(mask2d, 1, lx, ly, L, prm, monitor_every, radius, nsteps, fields,
+                         mon_out, nthreads);
+}
+
+// The same with a mask per core plane (lx*ly*L, 0 fluid / 125 wall): geometry that varies
+// along the pipe, such as wall roughness; buffer planes copy the wrapped core planes' masks.
+int oracle_run_core3d_f64(const uint8_t* mask3d, int lx, int ly, int L, const double* prm,
+                          int monitor_every, double radius, long nsteps, double* fields,
+                          double* mon_out, int nthreads) {
+  return run_core<double>(mask3d, L, lx, ly, L, prm, monitor_every, radius, nsteps, fields,
+                          mon_out, nthreads);
+}
+int oracle_run_core3d_f32(const uint8_t* mask3d, int lx, int ly, int L, const double* prm,
+                          int monitor_every, double radius, long nsteps, float* fields,
+                          double* mon_out, int nthreads) {
+  return run_core<float>(mask3d, L, lx, ly, L, prm, monitor_every, radius, nsteps, fields,
+                         mon_out, nthreads);
 }
 
 // Statistics accumulation of FSLBM.cu:715-748 on one sampled plane (n values per field).

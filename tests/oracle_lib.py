@@ -33,6 +33,8 @@ def lib():
         L.oracle_monitor_ref_f32.argtypes = [_u8p, i, i, i, i, d, d, _f32p, _f64p]
         L.oracle_run_core_f64.argtypes = [_u8p, i, i, i, _f64p, i, d, l, _f64p, ctypes.c_void_p, i]
         L.oracle_run_core_f32.argtypes = [_u8p, i, i, i, _f64p, i, d, l, _f32p, ctypes.c_void_p, i]
+        L.oracle_run_core3d_f64.argtypes = [_u8p, i, i, i, _f64p, i, d, l, _f64p, ctypes.c_void_p, i]
+        L.oracle_run_core3d_f32.argtypes = [_u8p, i, i, i, _f64p, i, d, l, _f32p, ctypes.c_void_p, i]
         L.oracle_stats_accumulate.argtypes = [l, _f64p, _f64p, _f64p, _f64p, i, _f64p]
         L.oracle_stats_accumulate.restype = None
         L.oracle_pipe_m_mask.argtypes = [i, i, i, _u8p]
@@ -83,14 +85,19 @@ def monitor_ref(io, fields, nu, radius, d2=10):
 
 def run_core(mask2d, L, fields, prm, nsteps, monitor_every=50, radius=0.0, dtype=np.float64,
              nthreads=0):
-    """Periodic-core run. mask2d (ly,lx) 0/125; fields (4,L,ly,lx). Returns (fields, monitor)."""
-    ly, lx = mask2d.shape
+    """Periodic-core run. mask2d (ly,lx) 0/125, or (L,ly,lx) for a mask per core plane;
+    fields (4,L,ly,lx). Returns (fields, monitor)."""
+    three_d = mask2d.ndim == 3
+    ly, lx = mask2d.shape[-2:]
     p = np.array([prm["tblend"], prm["pin"], prm["nu"], prm["d1"], prm["blend"],
                   *prm.get("force", (0.0, 0.0, 0.0)), prm.get("fd_order", 0)], np.float64)
     f = np.array(fields, dtype=dtype, order="C", copy=True)
     nmon = nsteps // monitor_every if monitor_every > 0 else 0
     mon = np.zeros((max(nmon, 1), 7))
-    fn = lib().oracle_run_core_f64 if dtype == np.float64 else lib().oracle_run_core_f32
+    if three_d:
+        fn = lib().oracle_run_core3d_f64 if dtype == np.float64 else lib().oracle_run_core3d_f32
+    else:
+        fn = lib().oracle_run_core_f64 if dtype == np.float64 else lib().oracle_run_core_f32
     rc = fn(np.ascontiguousarray(mask2d, np.uint8).ravel(), lx, ly, L, p, monitor_every,
             float(radius), nsteps, f.ravel(), mon.ctypes.data, nthreads or threads())
     if rc < 0:
