@@ -189,6 +189,51 @@ def cpu_port_sample(seconds=10.0, planes=64, nthreads=0):
                       f"the workload, oracle restatement of FSLBM.cu with OpenMP"}, el / steps
 
 
+def reference_gpu_sample(steps=20):
+    """The reference's own step kernels (FSLBMcalc, shiftback, bcond of FSLBM.cu) on this GPU,
+    built from the reference source with a texture-object compatibility header into
+    oracle/_ref (present only where the reference source was available at build time), on the
+    same pipe in the reference layout (10 buffer planes each end). MLUPS over the 512 core
+    planes, as the main metric counts. None when the library or a GPU is missing."""
+    import ctypes
+    path = os.path.join(ROOT, "oracle", "_ref", "libfslbm_ref.so")
+    try:
+        import torch
+        if not (os.path.exists(path) and torch.cuda.is_available()):
+            return None
+    except ImportError:
+        return None
+    import flowcontrast_b200 as fb
+    lib = ctypes.CDLL(path)
+    u8 = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+    f32 = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+    i = ctypes.c_int
+    lib.ref_run.argtypes = [u8, i, i, i, i, f32, f32, f32, i, ctypes.POINTER(ctypes.c_float),
+                            ctypes.POINTER(ctypes.c_uint)]
+    ub, umax, g = physics()
+    d2, L = 10, W["lz"]
+    dom = fb.make_domain(W["lx"], W["ly"], L, radius=W["R"], cx=W["cx"], cy=W["cy"])
+    core = fb.init_poiseuille(dom, umax, noise=1e-3, modes=4, mode_amp=0.1 * ub / umax,
+                              seed=W["seed"]).astype(np.float32)
+    f = np.concatenate([core[:, -d2:], core, core[:, :d2]], axis=1)
+    y, x = np.mgrid[0:W["ly"], 0:W["lx"]]
+    fluid = (x - W["cx"]) ** 2 + (y - W["cy"]) ** 2 <= W["R"] ** 2
+    io = np.where(fluid, 0, 125).astype(np.uint8)[None].repeat(L + 2 * d2, axis=0)
+    io[:d2][:, fluid] = 1
+    io[-d2:][:, fluid] = 1
+    prm = np.array([W["tblend"], 0.0, W["nu"], W["d1"], W["blend"]], np.float32)
+    out = np.empty_like(f)
+    ms, oob = ctypes.c_float(0), ctypes.c_uint(0)
+    rc = lib.ref_run(io, W["lx"], W["ly"], L + 2 * d2, d2, prm, np.ascontiguousarray(f).ravel(),
+                     out.ravel(), steps, ctypes.byref(ms), ctypes.byref(oob))
+    if rc != 0:
+        return {"unavailable": f"ref_run returned {rc}"}
+    cells = W["lx"] * W["ly"] * L
+    return {"value": cells * steps / (ms.value * 1e-3) / 1e6, "unit": "MLUPS", "steps": steps,
+            "kind": "the reference's FSLBMcalc/shiftback/bcond kernels on this GPU (CUDA-12 "
+                    "texture-object compatibility header), 512+2x10 planes, core cells counted"}
+
+
 def run_reference_arm(args, rank, world, local):
     """--impl reference: the reference method's CPU implementation (the oracle port) on the
     host cores, rank 0 only, on a bounded slice per step."""
@@ -231,7 +276,8 @@ def run_reference_arm(args, rank, world, local):
             "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "reference_gpu": reference_gpu_sample()}
     print(json.dumps(line), flush=True)
     return 0
 
