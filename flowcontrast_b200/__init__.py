@@ -35,7 +35,8 @@ class Domain(ctypes.Structure):
     _fields_ = [("lx", ctypes.c_int), ("ly", ctypes.c_int), ("lz", ctypes.c_int),
                 ("mask", ctypes.c_void_p), ("radius", ctypes.c_double),
                 ("cx", ctypes.c_double), ("cy", ctypes.c_double),
-                ("buffer_depth", ctypes.c_int), ("mask_planes", ctypes.c_int)]
+                ("buffer_depth", ctypes.c_int), ("mask_planes", ctypes.c_int),
+                ("periodic_xy", ctypes.c_int)]
 
 
 class Params(ctypes.Structure):
@@ -265,12 +266,14 @@ def ref_mask_to_core3d(mask3d, d2=10):
     return out
 
 
-def make_domain(lx, ly, lz, mask=None, radius=0.0, cx=None, cy=None, buffer_depth=10):
+def make_domain(lx, ly, lz, mask=None, radius=0.0, cx=None, cy=None, buffer_depth=10,
+                periodic_xy=0):
     """Domain struct; keeps a reference to the mask array on the struct. mask: (ly, lx) for a
-    cross-section extruded along z, or (lz, ly, lx) for one cross-section per plane."""
+    cross-section extruded along z, or (lz, ly, lx) for one cross-section per plane.
+    periodic_xy = G: cross-section periodic in x and y behind a G-wide ghost band."""
     d = Domain(lx, ly, lz, None, float(radius),
                float((lx - 1) / 2 if cx is None else cx), float((ly - 1) / 2 if cy is None else cy),
-               int(buffer_depth), 0)
+               int(buffer_depth), 0, int(periodic_xy))
     if mask is not None:
         m = np.ascontiguousarray(mask, np.uint8)
         if m.ndim == 3:

@@ -159,6 +159,9 @@ struct fslbm_solve {
   double l1 = 0;                   // the monitor's l1 (FSLBM.cu:589-591)
   int64_t fluid_total = 0;         // fluid cells of the core
   int planes = 1;                  // mask cross-sections: 1 (extruded) or L (one per plane)
+  int ghost = 0;                   // periodic cross-section: ghost band width (0: walls)
+  int2* d_ghosts = nullptr;        // (ghost cell, interior image) per ghost cell of a cross-section
+  int nghost = 0;
   int sx = 0, sy = 0, sz = 0;  // monitor sample cell
   // device
   void* state[2] = {nullptr, nullptr};
@@ -425,7 +428,7 @@ static void choose_chunks(fslbm_solve* s) {
 static void free_solve(fslbm_solve* s) {
   if (!s) return;
   cudaSetDevice(s->ctx->device);
-  void* ptrs[] = {s->state[0], s->state[1], s->d_mask, s->d_colcoef, s->d_tiles, s->d_counters,
+  void* ptrs[] = {s->state[0], s->state[1], s->d_mask, s->d_colcoef, s->d_tiles, s->d_ghosts, s->d_counters,
                   s->d_log, s->d_gauge, s->d_err, s->d_scratch, s->d_stats, s->d_prof,
                   s->d_stage, s->d_plane};
   for (void* p : ptrs) ctx_free(s->ctx, p);
@@ -473,6 +476,34 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
     return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: mask_planes must be 0, 1 or lz (%d) with a mask", dom->lz);
   }
   s->planes = dom->mask_planes > 1 ? dom->lz : 1;
+  // periodic cross-section: the band G cells wide at the rim takes the periodic images of the
+  // interior (2 where the image is fluid, 125 where it is wall)
+  std::vector<uint8_t> pmask;
+  if (dom->periodic_xy > 0) {
+    const int G = dom->periodic_xy, nx = dom->lx - 2 * G, ny = dom->ly - 2 * G;
+    double cf[9];
+    const int reach = fd_coefficients(prm->fd_order, prm->blend, dtype != FSLBM_F64, cf) * prm->d1;
+    if (s->planes > 1 || nx < 1 || ny < 1 || G < std::max(1, reach)) {
+      free_solve(s);
+      return fslbm_set_error(FSLBM_ERR_ARG,
+                             "solve_create: periodic_xy %d needs one cross-section, an interior of at "
+                             "least one cell and a band at least the corrector reach %d wide", G, reach);
+    }
+    s->ghost = G;
+    pmask.assign(size_t(dom->lx) * dom->ly, 0);
+    for (int y = 0; y < dom->ly; ++y)
+      for (int x = 0; x < dom->lx; ++x) {
+        const int sx = G + ((x - G) % nx + nx) % nx, sy = G + ((y - G) % ny + ny) % ny;
+        const uint8_t src = dom->mask ? dom->mask[size_t(sy) * dom->lx + sx] : uint8_t(0);
+        if (src != 0 && src != kWall) {
+          free_solve(s);
+          return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: mask value %d at (%d,%d); expected 0 or 125",
+                                 int(src), sx, sy);
+        }
+        const bool band = sx != x || sy != y;
+        pmask[size_t(y) * dom->lx + x] = band ? (src == kWall ? kWall : kGhost) : src;
+      }
+  }
   const size_t plane = size_t(s->lxp) * s->ly;
   s->mask.assign(plane * s->planes, kWall);
   std::vector<int64_t> per_plane(s->planes, 0);
@@ -481,7 +512,13 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
     for (int y = 0; y < s->ly; ++y)
       for (int x = 0; x < s->lx; ++x) {
         uint8_t v;
-        if (dom->mask) {
+        if (!pmask.empty()) {
+          v = pmask[size_t(y) * s->lx + x];
+          if (v != 0 && v != kWall && v != kGhost) {
+            free_solve(s);
+            return fslbm_set_error(FSLBM_ERR_ARG, "solve_create: mask value %d at (%d,%d); expected 0 or 125", v, x, y);
+          }
+        } else if (dom->mask) {
           v = dom->mask[(size_t(z) * s->ly + y) * s->lx + x];
           if (v != 0 && v != kWall) {
             free_solve(s);
@@ -581,6 +618,22 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
   if ((e = dalloc(s, &s->d_err, sizeof(unsigned)))) return fail("err");
   if ((e = cudaMemsetAsync(s->d_err, 0, sizeof(unsigned), st))) return fail("memset");
   if ((e = dalloc(s, &s->d_scratch, 8 * sizeof(double)))) return fail("scratch");
+  if (s->ghost > 0) {
+    const int G = s->ghost, nx = s->lx - 2 * G, ny = s->ly - 2 * G;
+    std::vector<int2> pairs;
+    for (int y = 0; y < s->ly; ++y)
+      for (int x = 0; x < s->lx; ++x) {
+        if (s->mask[size_t(y) * s->lxp + x] != kGhost) continue;
+        const int sx = G + ((x - G) % nx + nx) % nx, sy = G + ((y - G) % ny + ny) % ny;
+        pairs.push_back(make_int2(y * s->lxp + x, sy * s->lxp + sx));
+      }
+    s->nghost = int(pairs.size());
+    if ((e = dalloc(s, &s->d_ghosts, pairs.size() * sizeof(int2)))) return fail("ghosts");
+    if ((e = cudaMemcpyAsync(s->d_ghosts, pairs.data(), pairs.size() * sizeof(int2),
+                             cudaMemcpyHostToDevice, st)))
+      return fail("ghosts copy");
+    if ((e = cudaStreamSynchronize(st))) return fail("ghosts copy");   // pairs is a local vector
+  }
   if ((e = cudaEventCreate(&s->ev0)) || (e = cudaEventCreate(&s->ev1))) return fail("events");
   if (int r = configure_kernel(s)) { free_solve(s); return r; }
   *out = s;
@@ -646,6 +699,7 @@ extern "C" int fslbm_solve_set_fields(fslbm_solve* s, fslbm_dtype hd, const void
                                s->L, st));
   }
   CUDA_TRY(launch_zero_walls(s->dtype, dst, s->d_mask, s->planes, s->lxp, s->ly, s->L, st));
+  CUDA_TRY(launch_fill_ghosts(s->dtype, dst, s->d_ghosts, s->nghost, s->lxp, s->ly, s->L, st));
   // the other buffer's walls (never written by the step) must be zero too
   CUDA_TRY(launch_zero_walls(s->dtype, s->state[1 - s->cur], s->d_mask, s->planes, s->lxp, s->ly, s->L, st));
   s->fields_set = true;
@@ -675,6 +729,8 @@ extern "C" int fslbm_solve_init_poiseuille(fslbm_solve* s, double umax, double n
   CUDA_TRY(cudaSetDevice(s->ctx->device));
   cudaStream_t st = s->ctx->stream;
   CUDA_TRY(launch_init_poiseuille(s->dtype, s->state[s->cur], s->d_mask, s->planes, s->lxp, q, st));
+  CUDA_TRY(launch_fill_ghosts(s->dtype, s->state[s->cur], s->d_ghosts, s->nghost, s->lxp, s->ly,
+                              s->L, st));
   CUDA_TRY(launch_zero_walls(s->dtype, s->state[1 - s->cur], s->d_mask, s->planes, s->lxp, s->ly, s->L, st));
   s->fields_set = true;
   return FSLBM_OK;
@@ -797,6 +853,10 @@ static int enqueue_steps(fslbm_solve* s, int64_t nsteps) {
       s->tev_used += 2;
     }
     ++s->launches;
+    if (s->nghost) {                 // periodic cross-section: refresh the ghost band
+      CUDA_TRY(launch_fill_ghosts(s->dtype, a.out, s->d_ghosts, s->nghost, s->lxp, s->ly, s->L, st));
+      ++s->launches;
+    }
     s->cur ^= 1;
     s->steps = c;
     if (me > 0 && c % me == 0) {
@@ -1341,7 +1401,7 @@ extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, in
     b->m_chunk.push_back(64);
     b->m_w4.push_back(1);
     fast = fast && solves[i]->use2 && solves[i]->ty2 == 32 && solves[i]->prm.d1 == 2 &&
-           solves[i]->dtype == solves[0]->dtype;
+           solves[i]->dtype == solves[0]->dtype && solves[i]->nghost == 0;
   }
   b->fast = fast;
   default_tiling(b);

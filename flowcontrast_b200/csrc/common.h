@@ -8,6 +8,7 @@ constexpr int kTX = 32;                 // step tile width along x (one warp per
 constexpr int kTY = 8;                  // step tile height along y
 constexpr int kThreads = kTX * kTY;
 constexpr uint8_t kWall = 125;          // mask value of a wall cell (pipe.m:45-47)
+constexpr uint8_t kGhost = 2;           // periodic image cell of a cross-section periodic in x, y
 
 // Per cross-section column: static wall sums of the predictor and the fluid flag.
 template <class TC> struct ColCoef {

@@ -98,6 +98,9 @@ cudaError_t launch_batch_monitor(const BatchMon* mons, int n, int parity_after, 
 // Seeded Poiseuille start written into a pitched state (walls and pad columns zero).
 cudaError_t launch_init_poiseuille(int dtype, void* state, const uint8_t* mask, int planes, int lxp,
                                    const PoiseuilleInit& q, cudaStream_t st);
+// Periodic cross-section: pairs (ghost cell, interior image) as cross-section indices.
+cudaError_t launch_fill_ghosts(int dtype, void* state, const int2* pairs, int n, int lxp, int ly,
+                               int L, cudaStream_t st);
 // masks: `planes` cross-sections of lxp*ly bytes (1: extruded along z)
 cudaError_t launch_zero_walls(int dtype, void* state, const uint8_t* mask, int planes, int lxp,
                               int ly, int L, cudaStream_t st);

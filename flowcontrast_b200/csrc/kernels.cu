@@ -1,5 +1,6 @@
 // Kernel launchers and the small auxiliary kernels of the solve runtime (monitor reduction,
 // statistics accumulation, field conversion, divergence check).
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include "internal.h"
@@ -203,10 +204,11 @@ __device__ void monitor_body(const MonitorLaunch& a, double* sh) {
   const TA pin = TA(a.pin);
   double v[3] = {0, 0, 0};   // sum w, sum p, sum (p - pin) over non-wall cells of plane z=0
   for (int j = threadIdx.x; j < a.lxp * a.ly; j += blockDim.x) {
+    if (a.mask[j] != 0) continue;           // walls hold zero; periodic images are not counted
     const TA p = TA(st[j]);
     v[0] += to_d(st[3 * FS + j]);
     v[1] += double(p);
-    if (a.mask[j] != kWall) v[2] += double(TA(p - pin));   // the outlet buffer copy's p
+    v[2] += double(TA(p - pin));            // the outlet buffer copy's p
   }
   block_sum<3>(v, sh);
   if (threadIdx.x == 0) {
@@ -359,6 +361,36 @@ cudaError_t launch_init_poiseuille(int dtype, void* state, const uint8_t* mask, 
     init_poiseuille_kernel<double><<<grid, 256, 0, st>>>((double*)state, mask, planes, lxp, q);
   else if (dtype == FSLBM_F16)
     init_poiseuille_kernel<__half><<<grid, 256, 0, st>>>((__half*)state, mask, planes, lxp, q);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------
+// periodic cross-section: ghost cells take their interior images (every plane, four fields)
+// ------------------------------------------------------------------------------------------
+template <class TS>
+__global__ void fill_ghosts_kernel(TS* s, const int2* pairs, int n, size_t plane, int L) {
+  const size_t FS = plane * L;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < size_t(n) * L;
+       i += size_t(gridDim.x) * blockDim.x) {
+    const int2 pr = pairs[i % n];
+    const size_t z = (i / n) * plane, d = z + pr.x, sidx = z + pr.y;
+    s[d] = s[sidx]; s[FS + d] = s[FS + sidx]; s[2 * FS + d] = s[2 * FS + sidx];
+    s[3 * FS + d] = s[3 * FS + sidx];
+  }
+}
+
+cudaError_t launch_fill_ghosts(int dtype, void* state, const int2* pairs, int n, int lxp, int ly,
+                               int L, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const size_t plane = size_t(lxp) * ly;
+  const int grid = int(std::min<size_t>(1184, (size_t(n) * L + 255) / 256));
+  if (dtype == FSLBM_F32)
+    fill_ghosts_kernel<float><<<grid, 256, 0, st>>>((float*)state, pairs, n, plane, L);
+  else if (dtype == FSLBM_F64)
+    fill_ghosts_kernel<double><<<grid, 256, 0, st>>>((double*)state, pairs, n, plane, L);
+  else if (dtype == FSLBM_F16)
+    fill_ghosts_kernel<__half><<<grid, 256, 0, st>>>((__half*)state, pairs, n, plane, L);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }

@@ -65,6 +65,12 @@ typedef struct {
                             kernel, FP32/FP64). The monitor's l1, the reference's buffer-cell
                             count over 2*d2 planes (FSLBM.cu:589-591), is then the mean fluid
                             count of the buffer_depth planes at each end of the core. */
+  int periodic_xy;       /* addition: G > 0 makes the cross-section periodic in x and y with
+                            period (lx - 2G, ly - 2G): a G-wide band at the box rim holds the
+                            periodic images of the interior (mask value 2; refilled after every
+                            step, never stepped, not counted by monitors). G >= K*d1, one
+                            cross-section only. A given mask's band values are replaced; without
+                            a mask the interior is all fluid (e.g. a Taylor-Green vortex). */
 } fslbm_domain;
 
 /* Run parameters: the six lines of param.txt (FSLBM.cu:502-507) plus additions. */

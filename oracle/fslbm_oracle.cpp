@@ -46,6 +46,7 @@ namespace {
 
 constexpr int WALL = 125;
 constexpr int BUF = 1;
+constexpr int GHOST = 2;   // addition: periodic image cell of a cross-section periodic in x and y
 
 template <class T> struct Consts {
   T tb, cc, pin, dtddy, m, c0, c1, c2, gauge, fx, fy, fz;
@@ -262,7 +263,7 @@ void pad_core(const uint8_t* mask, int planes, int lx, int ly, int L, int d2, T 
     for (long j = 0; j < lxy; ++j) {
       const long r = j + lxy * z, c = j + lxy * zc;
       const bool wall = mp[j] == WALL;
-      io[r] = wall ? WALL : (jump ? BUF : 0);
+      io[r] = wall ? WALL : (mp[j] == GHOST ? GHOST : (jump ? BUF : 0));
       if (wall) continue;
       T pv = core[c];
       if (jump == 1) pv += pin;
@@ -284,6 +285,7 @@ void monitor_ref(const uint8_t* io, int lx, int ly, int lz, int d2, double nu, d
   l1 /= double(2 * d2);                                       // FSLBM.cu:589-591
   double q1 = 0, q2 = 0, p1 = 0, p2 = 0;
   for (long j = 0; j < lxy; ++j) {
+    if (io[j + lxy * d2] == GHOST) continue;                   // periodic images are not counted
     q2 += double(f[3 * n + j + lxy * (lz - d2)]); p2 += double(f[j + lxy * (lz - d2)]);
     q1 += double(f[3 * n + j + lxy * d2]);        p1 += double(f[j + lxy * d2]);
   }
@@ -295,10 +297,27 @@ void monitor_ref(const uint8_t* io, int lx, int ly, int lz, int d2, double nu, d
   out[6] = 2.0 * radius * q1 / nu;                            // FSLBM.cu:650
 }
 
+// Refills the ghost band (cells marked GHOST, G wide) of a cross-section periodic in x and y
+// with the periodic images of the interior, in every plane of the core fields.
+template <class T>
+void fill_ghosts(const uint8_t* mask2d, int lx, int ly, int L, int G, T* fields) {
+  if (G <= 0) return;
+  const int nx = lx - 2 * G, ny = ly - 2 * G;
+  const long lxy = long(lx) * ly, nc = lxy * L;
+  for (int y = 0; y < ly; ++y)
+    for (int x = 0; x < lx; ++x) {
+      if (mask2d[x + long(lx) * y] != GHOST) continue;
+      const int sx = G + ((x - G) % nx + nx) % nx, sy = G + ((y - G) % ny + ny) % ny;
+      for (int k = 0; k < 4; ++k)
+        for (int z = 0; z < L; ++z)
+          fields[k * nc + lxy * z + x + long(lx) * y] = fields[k * nc + lxy * z + sx + long(lx) * sy];
+    }
+}
+
 template <class T>
 int run_core(const uint8_t* mask2d, int planes, int lx, int ly, int L, const double* prm,
              int monitor_every, double radius, long nsteps, T* fields, double* mon_out,
-             int nthreads) {
+             int nthreads, int ghost = 0) {
   // prm: tblend, pin, nu, d1, blend, fx, fy, fz, fd_order (gauge is driven here)
   const int d1 = int(prm[3]);
   double cdum[9];
@@ -311,7 +330,7 @@ int run_core(const uint8_t* mask2d, int planes, int lx, int ly, int L, const dou
     for (int y = 0; y < ly; ++y)
       for (int x = 0; x < lx; ++x) {
         const uint8_t c = mask2d[x + long(lx) * (y + long(ly) * z)];
-        if (c != 0 && c != WALL) return -2;
+        if (c != 0 && c != WALL && !(c == GHOST && ghost > 0)) return -2;
         if (c == 0 && (x == 0 || y == 0 || x == lx - 1 || y == ly - 1)) return -4;
       }
   const long nc = long(lx) * ly * L, lxy = long(lx) * ly;
@@ -329,6 +348,7 @@ int run_core(const uint8_t* mask2d, int planes, int lx, int ly, int L, const dou
     const long nr = long(lx) * ly * lz;
     for (int k = 0; k < 4; ++k)
       std::memcpy(fields + k * nc, b.data() + k * nr + lxy * d2, sizeof(T) * nc);
+    fill_ghosts(mask2d, lx, ly, L, ghost, fields);
     if (monitor_every > 0 && c % monitor_every == 0) {
       double m[7];
       monitor_ref<T>(io.data(), lx, ly, lz, d2, prm[2], radius, b.data(), m);
@@ -392,6 +412,25 @@ int oracle_run_core_f32(const uint8_t* mask2d, int lx, int ly, int L, const doub
                         double* mon_out, int nthreads) {
   return run_core<float>(mask2d, 1, lx, ly, L, prm, monitor_every, radius, nsteps, fields,
                          mon_out, nthreads);
+}
+
+// The same with a cross-section periodic in x and y (an addition, not in the reference): a band
+// of `ghost` cells at the box rim, marked 2 in mask2d, holds the periodic images of the interior
+// (period lx - 2*ghost by ly - 2*ghost); ghosts are read as fluid neighbours, never stepped, and
+// refilled after every step; monitors skip them.
+int oracle_run_core_periodic_f64(const uint8_t* mask2d, int lx, int ly, int L, int ghost,
+                                 const double* prm, int monitor_every, double radius, long nsteps,
+                                 double* fields, double* mon_out, int nthreads) {
+  fill_ghosts(mask2d, lx, ly, L, ghost, fields);
+  return run_core<double>(mask2d, 1, lx, ly, L, prm, monitor_every, radius, nsteps, fields,
+                          mon_out, nthreads, ghost);
+}
+int oracle_run_core_periodic_f32(const uint8_t* mask2d, int lx, int ly, int L, int ghost,
+                                 const double* prm, int monitor_every, double radius, long nsteps,
+                                 float* fields, double* mon_out, int nthreads) {
+  fill_ghosts(mask2d, lx, ly, L, ghost, fields);
+  return run_core<float>(mask2d, 1, lx, ly, L, prm, monitor_every, radius, nsteps, fields,
+                         mon_out, nthreads, ghost);
 }
 
 // The same with a mask per core plane (lx*ly*L, 0 fluid / 125 wall): geometry that varies

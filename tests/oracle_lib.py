@@ -35,6 +35,10 @@ def lib():
         L.oracle_run_core_f32.argtypes = [_u8p, i, i, i, _f64p, i, d, l, _f32p, ctypes.c_void_p, i]
         L.oracle_run_core3d_f64.argtypes = [_u8p, i, i, i, _f64p, i, d, l, _f64p, ctypes.c_void_p, i]
         L.oracle_run_core3d_f32.argtypes = [_u8p, i, i, i, _f64p, i, d, l, _f32p, ctypes.c_void_p, i]
+        L.oracle_run_core_periodic_f64.argtypes = [_u8p, i, i, i, i, _f64p, i, d, l, _f64p,
+                                                   ctypes.c_void_p, i]
+        L.oracle_run_core_periodic_f32.argtypes = [_u8p, i, i, i, i, _f64p, i, d, l, _f32p,
+                                                   ctypes.c_void_p, i]
         L.oracle_stats_accumulate.argtypes = [l, _f64p, _f64p, _f64p, _f64p, i, _f64p]
         L.oracle_stats_accumulate.restype = None
         L.oracle_pipe_m_mask.argtypes = [i, i, i, _u8p]
@@ -118,3 +122,34 @@ def fd_coefficients(order, blend=0.0):
     if k == 0:
         raise ValueError(f"no corrector of order {order}")
     return c[:k + 1]
+
+
+def periodic_mask(nx, ny, G, inner=None):
+    """Cross-section periodic in x and y: interior nx x ny (0 fluid / 125 wall, all fluid by
+    default) inside a G-wide ghost band (2 where the periodic image is fluid)."""
+    lx, ly = nx + 2 * G, ny + 2 * G
+    inner = np.zeros((ny, nx), np.uint8) if inner is None else np.asarray(inner, np.uint8)
+    m = np.empty((ly, lx), np.uint8)
+    for y in range(ly):
+        for x in range(lx):
+            v = inner[(y - G) % ny, (x - G) % nx]
+            inside = G <= x < lx - G and G <= y < ly - G
+            m[y, x] = v if inside else (125 if v == 125 else 2)
+    return m
+
+
+def run_periodic(mask2d, L, G, fields, prm, nsteps, monitor_every=0, radius=0.0,
+                 dtype=np.float64, nthreads=0):
+    """Periodic-core run with a cross-section periodic in x and y (ghost band G)."""
+    ly, lx = mask2d.shape
+    p = np.array([prm["tblend"], prm["pin"], prm["nu"], prm["d1"], prm["blend"],
+                  *prm.get("force", (0.0, 0.0, 0.0)), prm.get("fd_order", 0)], np.float64)
+    f = np.array(fields, dtype=dtype, order="C", copy=True)
+    nmon = nsteps // monitor_every if monitor_every > 0 else 0
+    mon = np.zeros((max(nmon, 1), 7))
+    fn = lib().oracle_run_core_periodic_f64 if dtype == np.float64 else lib().oracle_run_core_periodic_f32
+    rc = fn(np.ascontiguousarray(mask2d, np.uint8).ravel(), lx, ly, L, G, p, monitor_every,
+            float(radius), nsteps, f.ravel(), mon.ctypes.data, nthreads or threads())
+    if rc < 0:
+        raise ValueError(f"oracle_run_core_periodic rejected the case: code {rc}")
+    return f, mon[:nmon]
