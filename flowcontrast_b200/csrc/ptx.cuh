@@ -64,6 +64,17 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// Shared-memory counter add with acquire-release semantics at CTA scope: accesses before it (in
+// this thread, and in threads that synchronised with it) are ordered before it, and the adds to
+// one counter form a release sequence, so the thread whose add completes a count is ordered
+// after every earlier adder's prior accesses. Returns the previous value.
+__device__ __forceinline__ uint32_t atom_add_acq_rel_cta(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], %2;"
+               : "=r"(old) : "r"(smem_u32(p)), "r"(v) : "memory");
+  return old;
+}
+
 // 4-D tiled TMA load into this CTA's shared memory, completion counted on `bar`.
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar,
                                             int c0, int c1, int c2, int c3) {

@@ -8,9 +8,11 @@
 //  - a 32 x TY tile per CTA (512 threads for TY = 32, 16 warps per SM); p is staged with a
 //    one-cell halo, u,v,w with the corrector's 2*d1 halo, as two TMA boxes per plane into a
 //    window of 8 planes (output plane .. 3 planes ahead for d1 = 2);
-//  - no block-wide barrier in the march: per-slot "full" mbarriers (TMA completion) and
-//    "empty" mbarriers (one arrival per warp after its last read of a plane) pace one producer
-//    thread, so warps drift within the window;
+//  - no block-wide barrier in the march: per-slot "full" mbarriers count TMA completion, and
+//    each warp releases a slot after its last read of the plane in it, so warps drift within
+//    the window. The single-pipe kernel lets the last warp to release a slot refill it (no warp
+//    waits for a free slot); the batched kernel has thread 0 wait on per-slot "empty"
+//    mbarriers and refill;
 //  - the streamwise corrector taps behind the output plane come from a 2*d1 register history
 //    of the thread's own columns, the taps ahead from the window;
 //  - grid = tiles x streamwise chunks in chunk-major order, so concurrent CTAs work at nearby
@@ -53,7 +55,8 @@ template <int D1, int TY, class TE = float> struct Step2Tile {
   static constexpr uint32_t TX_BYTES = uint32_t((SW * PH + 3 * UPLANE) * ES);
   static constexpr size_t RING_BYTES = size_t(S) * SLOT * ES;
   static constexpr size_t BAR_OFFSET = RING_BYTES;
-  static constexpr size_t SMEM_BYTES = BAR_OFFSET + 2 * S * sizeof(uint64_t);
+  // full and empty mbarriers per slot, then a release counter per slot
+  static constexpr size_t SMEM_BYTES = BAR_OFFSET + 2 * S * sizeof(uint64_t) + S * sizeof(uint32_t);
   static_assert((PPLANE * ES) % 128 == 0 && (UPLANE * ES) % 16 == 0 && (SLOT * ES) % 128 == 0,
                 "TMA destinations must stay aligned");
   static_assert((HX * ES) % 16 == 0, "TMA box x start must be 16-byte aligned");
@@ -172,7 +175,11 @@ __device__ __forceinline__ float2 qof(float2 P, float2 U, float2 V, float2 W) {
 // Marches one (tile, chunk) work item of one pipe: the step of every cell of the tile's columns
 // in the chunk's planes. `reinit` re-arms the CTA's mbarriers when the CTA has marched an item
 // before (persistent grids). Returns false when a bounded wait gave up (error flag set).
-template <int D1, int TY, bool PK, class TE, bool W16X4 = false>
+// REFILL_LAST selects how freed window slots are refilled: by the last warp to release the slot
+// (no warp waits; +2 % on the single-pipe kernel) or by thread 0, which waits on the slot's empty
+// mbarrier (fewer live registers: the batched kernel, whose member state already presses on the
+// register budget, is 1 % faster this way).
+template <int D1, int TY, bool PK, class TE, bool W16X4 = false, bool REFILL_LAST = false>
 __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUtensorMap* tmap_uvw,
                                             const Step2Geom& g, const StepConst<float>& k,
                                             int tile, int chunk, unsigned char* smem, bool reinit) {
@@ -184,7 +191,9 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
 
   TE* ring = reinterpret_cast<TE*>(smem);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + Tl::BAR_OFFSET);
-  uint64_t* empty = full + S;
+  uint64_t* empty = full + S;     // per slot: one arrival per warp after its last read (thread 0 refills)
+  // per slot: warp releases, counted to elect the refilling warp (last-warp refill)
+  unsigned* released = reinterpret_cast<unsigned*>(empty + S);
 
   // Warp shape. Default: 32 columns x 2 rows (each half-warp reads one contiguous row).
   // W16X4: 16 columns (8 pairs) x 4 rows, so warps over wall skip at a finer grain, which pays
@@ -219,9 +228,15 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
   __syncthreads();   // a previous item (persistent grids) is fully consumed
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
-      if (reinit) { mbar_inval(&full[s]); mbar_inval(&empty[s]); }
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], Tl::WARPS);
+      if constexpr (REFILL_LAST) {
+        if (reinit) mbar_inval(&full[s]);
+        mbar_init(&full[s], 1);
+        released[s] = 0u;
+      } else {
+        if (reinit) { mbar_inval(&full[s]); mbar_inval(&empty[s]); }
+        mbar_init(&full[s], 1);
+        mbar_init(&empty[s], Tl::WARPS);
+      }
     }
     mbar_init_fence();
   }
@@ -236,16 +251,31 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
     tma_load_4d(dst, tmap_p, &full[slot], org.x - HX, org.y - 1, zz, 0);
     tma_load_4d(dst + PPL, tmap_uvw, &full[slot], org.x - HX, org.y - HY, zz, 1);
   };
-  int issued = -1;                                            // last march plane issued (thread 0)
+  // Thread 0 loads the first planes: the whole ring (last-warp refill), or the output plane and
+  // AH planes ahead (thread-0 refill, which keeps the slots of planes m - R .. m - 1 for the
+  // corrector's taps behind).
+  int issued = -1;                                          // thread-0 refill: last plane issued
   if (tid == 0) {
     prefetch_tensormap(tmap_p);
     prefetch_tensormap(tmap_uvw);
-    for (int m = 0; m <= AH && m < niter; ++m) { issue(m); issued = m; }
+    if constexpr (REFILL_LAST) {
+      for (int m = 0; m < S && m < niter; ++m) issue(m);
+    } else {
+      for (int m = 0; m <= AH && m < niter; ++m) { issue(m); issued = m; }
+    }
   }
-  auto drain = [&](int from) {                                // failure path: let loads land
-    if (tid == 0)
-      for (int q = from; q <= issued; ++q)
-        mbar_wait_bounded(&full[q & (S - 1)], uint32_t((q / S) & 1), kWaitLimitNs / 8);
+  // failure path: let loads in flight land (bounded) before returning. With the last-warp refill
+  // any warp may have issued up to S planes ahead; otherwise thread 0 knows what it issued.
+  auto drain = [&](int from) {
+    if constexpr (REFILL_LAST) {
+      if (lane == 0)
+        for (int q = from; q < niter && q < from + S; ++q)
+          mbar_wait_bounded(&full[q & (S - 1)], uint32_t((q / S) & 1), kWaitLimitNs / 8);
+    } else {
+      if (tid == 0)
+        for (int q = from; q <= issued; ++q)
+          mbar_wait_bounded(&full[q & (S - 1)], uint32_t((q / S) & 1), kWaitLimitNs / 8);
+    }
   };
   // wait for march plane m; false after flagging a failure (the caller returns)
   auto arrive_wait = [&](int m) -> bool {
@@ -254,21 +284,40 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
     drain(m + 1);
     return false;
   };
-  // plane m - R leaves the window: release its slot; thread 0 refills it with plane m + AH + 1
+  // Plane m - R leaves the window and its slot takes plane m - R + S (= m + AH + 1).
+  // Last-warp refill: __syncwarp orders the warp's shared loads before lane 0's acq_rel add to the
+  // slot's counter; the warp whose add completes the count has acquired every warp's loads and
+  // orders them before its TMA write with a proxy fence. A slot's next cycle starts only after
+  // its refill lands, which needs all WARPS releases of this cycle, so the count is a multiple
+  // of WARPS exactly when a cycle is complete.
+  // Thread-0 refill: each warp arrives on the slot's empty mbarrier (release semantics) and
+  // thread 0 waits on it (acquire) before the proxy fence and the TMA.
   auto release_produce = [&](int m) -> bool {
     __syncwarp();
-    if (m >= R && lane == 0) mbar_arrive(&empty[(m - R) & (S - 1)]);
-    if (tid == 0 && m + AH + 1 < niter) {
-      const int mn = m + AH + 1;
-      if (mn >= S &&
-          !mbar_wait_bounded(&empty[mn & (S - 1)], uint32_t(((mn - S) / S) & 1), kWaitLimitNs)) {
-        atomicOr(g.err, 1u);
-        drain(m + 1);
-        return false;
+    if constexpr (REFILL_LAST) {
+      if (m >= R && lane == 0) {
+        const int slot = (m - R) & (S - 1);
+        const unsigned seen = atom_add_acq_rel_cta(&released[slot], 1u) + 1u;
+        const int mn = m - R + S;
+        if (seen % unsigned(Tl::WARPS) == 0u && mn < niter) {
+          fence_proxy_async_smem();
+          issue(mn);
+        }
       }
-      fence_proxy_async_smem();
-      issue(mn);
-      issued = mn;
+    } else {
+      if (m >= R && lane == 0) mbar_arrive(&empty[(m - R) & (S - 1)]);
+      if (tid == 0 && m + AH + 1 < niter) {
+        const int mn = m + AH + 1;
+        if (mn >= S &&
+            !mbar_wait_bounded(&empty[mn & (S - 1)], uint32_t(((mn - S) / S) & 1), kWaitLimitNs)) {
+          atomicOr(g.err, 1u);
+          drain(m + 1);
+          return false;
+        }
+        fence_proxy_async_smem();
+        issue(mn);
+        issued = mn;
+      }
     }
     return true;
   };
@@ -508,7 +557,7 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
                        const StepConst<float> k) {
   extern __shared__ __align__(128) unsigned char smem[];
   if (threadIdx.x == 0 && blockIdx.x == 0 && g.step_counter) *g.step_counter += 1;
-  step2_march<D1, TY, PK, TE>(&tmap_p, &tmap_uvw, g, k, blockIdx.x % g.ntiles,
+  step2_march<D1, TY, PK, TE, false, true>(&tmap_p, &tmap_uvw, g, k, blockIdx.x % g.ntiles,
                           blockIdx.x / g.ntiles, smem, false);
 }
 
