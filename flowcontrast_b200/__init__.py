@@ -509,6 +509,12 @@ class Batch:
             _check(lib().fslbm_batch_destroy(self.handle))
             self.handle = None
 
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
 
 class Server:
     """Served solves with continuous batching (fslbm_server_*): its own context and worker

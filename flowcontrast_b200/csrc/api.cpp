@@ -2,6 +2,7 @@
 // ensemble and the device-side monitor log. The reference keeps all of this in main()
 // (FSLBM.cu:489-905); here it is a library with explicit error codes.
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
 #include <cstdarg>
@@ -59,12 +60,27 @@ extern "C" int fslbm_last_error(char* buf, size_t n) {
 // pool, which keeps freed blocks (release threshold: never), so creating and destroying solves
 // in a serving loop neither maps nor unmaps device memory nor synchronises the device. All
 // set-up copies run on the context's stream, behind the allocations.
+// A context is reference-counted: the creator holds one reference and every live solve and
+// batch one more, so destroying the context before its solves (an error path, or objects
+// finalised in any order at interpreter exit) defers the teardown to the last of them.
 struct fslbm_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaMemPool_t pool = nullptr;
   int sm_count = 0;
+  std::atomic<int> refs{1};
 };
+
+static void ctx_retain(fslbm_ctx* c) { c->refs.fetch_add(1); }
+
+static void ctx_release(fslbm_ctx* c) {
+  if (c->refs.fetch_sub(1) != 1) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  cudaMemPoolDestroy(c->pool);
+  cudaStreamDestroy(c->stream);
+  delete c;
+}
 
 static cudaError_t ctx_alloc(fslbm_ctx* c, void** p, size_t bytes) {
   return cudaMallocFromPoolAsync(p, std::max<size_t>(bytes, 1), c->pool, c->stream);
@@ -112,12 +128,7 @@ extern "C" int fslbm_ctx_create(int device, fslbm_ctx** out) {
 }
 
 extern "C" int fslbm_ctx_destroy(fslbm_ctx* c) {
-  if (!c) return FSLBM_OK;
-  cudaSetDevice(c->device);
-  cudaStreamSynchronize(c->stream);
-  cudaMemPoolDestroy(c->pool);
-  cudaStreamDestroy(c->stream);
-  delete c;
+  if (c) ctx_release(c);
   return FSLBM_OK;
 }
 
@@ -435,7 +446,9 @@ static void free_solve(fslbm_solve* s) {
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
   for (cudaEvent_t e : s->tev) cudaEventDestroy(e);
+  fslbm_ctx* c = s->ctx;
   delete s;
+  ctx_release(c);
 }
 
 template <class T>
@@ -465,6 +478,7 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
 
   auto* s = new fslbm_solve;
   s->ctx = ctx;
+  ctx_retain(ctx);
   s->lx = dom->lx; s->ly = dom->ly; s->L = dom->lz;
   s->lxp = (dom->lx + 7) / 8 * 8;
   s->d2 = dom->buffer_depth;
@@ -1206,7 +1220,9 @@ static void free_batch(fslbm_batch* b) {
   ctx_free(b->ctx, b->d_tickets);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
+  fslbm_ctx* c = b->ctx;
   delete b;
+  ctx_release(c);
 }
 
 // Work of one (tile, chunk) item of the column-pair kernel, for ordering the items: planes
@@ -1390,6 +1406,7 @@ extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, in
   if (!ctx || !out || n < 1 || !solves) return fslbm_set_error(FSLBM_ERR_ARG, "batch_create: bad argument");
   auto* b = new fslbm_batch;
   b->ctx = ctx;
+  ctx_retain(ctx);
   bool fast = true;
   for (int i = 0; i < n; ++i) {
     if (!solves[i] || solves[i]->ctx != ctx) {

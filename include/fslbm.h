@@ -117,6 +117,9 @@ int fslbm_last_error(char* buf, size_t n);
 
 /* ---- context: one device, one stream (replaces cudaSetDevice(0), FSLBM.cu:490) ---- */
 int fslbm_ctx_create(int device, fslbm_ctx** out);
+/* Drops the creator's reference. Each solve and batch holds its own, so the stream and memory
+   pool are released when the last of the context, its solves and its batches is destroyed
+   (any order is safe). */
 int fslbm_ctx_destroy(fslbm_ctx* ctx);
 
 /* ---- solve (replaces main's set-up and time loop, FSLBM.cu:489-905) ---- */
