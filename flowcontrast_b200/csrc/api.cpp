@@ -1184,9 +1184,10 @@ extern "C" int fslbm_profile_reset(fslbm_solve* s) {
 }
 
 // ------------------------------------------------------------------------------------------
-// batched ensemble: all members' steps of one time step in one persistent launch (FP32,
-// d1 = 2), followed by one bookkeeping launch (step counters, monitors, gauges); two steps are
-// captured once as a CUDA graph and replayed. Members of other kinds step one after another.
+// batched ensemble: `chain` time steps of all members in one persistent launch (FP32 or FP16
+// storage, d1 = 2), steps chained per member inside the launch (step counters, monitors and
+// gauges booked there too); the launch is captured once as a CUDA graph and replayed. Members
+// of other kinds step one after another.
 // ------------------------------------------------------------------------------------------
 struct fslbm_batch {
   fslbm_ctx* ctx = nullptr;
@@ -1196,16 +1197,18 @@ struct fslbm_batch {
   void* d_members = nullptr;
   BatchMon* d_mons = nullptr;
   int2* d_items = nullptr;         // (member, item of the member), longest first
-  unsigned* d_tickets = nullptr;   // [0..1] work-item counters per step parity, [2] error flag
+  unsigned* d_tickets = nullptr;   // [2] the batch's error flag ([0], [1], [3] unused)
+  unsigned* d_sync = nullptr;      // counters of the chained launch (batch_sync_words)
+  int chain = 16;                  // steps per chained launch (and per graph replay)
   std::vector<unsigned char> h_members;
   std::vector<BatchMon> h_mons;
   std::vector<int2> h_items;
   int nitems = 0, grid = 0, packed = 1;
   // per member tiling: streamwise planes per work item and warp shape (16 x 4 or 32 x 2),
-  // from the tuning table by size class, else 64 (FSLBM_BATCH_CHUNK) and 16 x 4
+  // from the tuning table by size class, else 128 (FSLBM_BATCH_CHUNK) and 16 x 4
   std::vector<int> m_chunk, m_w4;
   int shrink = 1;                  // chunk divisor for batches with fewer than 2 items per SM
-  cudaGraphExec_t exec2 = nullptr;
+  cudaGraphExec_t exec2 = nullptr;  // one chained launch of `chain` steps
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
 };
@@ -1218,6 +1221,7 @@ static void free_batch(fslbm_batch* b) {
   ctx_free(b->ctx, b->d_mons);
   ctx_free(b->ctx, b->d_items);
   ctx_free(b->ctx, b->d_tickets);
+  ctx_free(b->ctx, b->d_sync);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   fslbm_ctx* c = b->ctx;
@@ -1314,11 +1318,11 @@ static int batch_upload(fslbm_batch* b) {
   return FSLBM_OK;
 }
 
-static cudaError_t batch_enqueue_one(fslbm_batch* b, int parity, cudaStream_t st) {
-  cudaError_t e = launch_batch_step(b->members[0]->dtype, b->d_members, b->d_items, b->nitems,
-                                    b->grid, parity, b->packed, b->d_tickets, st);
-  if (e) return e;
-  return launch_batch_monitor(b->d_mons, int(b->members.size()), parity ^ 1, b->d_tickets, st);
+// One chained launch of `nsteps` steps for every member (each starting at its buffer cur0).
+static cudaError_t batch_enqueue(fslbm_batch* b, int nsteps, cudaStream_t st) {
+  return launch_batch_steps(b->members[0]->dtype, b->d_members, b->d_mons, b->d_items, b->nitems,
+                            nsteps, b->grid, b->packed, b->d_sync, int(b->members.size()),
+                            b->d_tickets + 2, st);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1334,7 +1338,7 @@ static std::string class_key(const fslbm_solve* s) {
   return buf;
 }
 
-struct Tiling { int chunk = 64, w16x4 = 1; double ms = 0; };
+struct Tiling { int chunk = 128, w16x4 = 1; double ms = 0; };
 using TilingTable = std::map<std::string, Tiling>;
 
 static bool write_tiling(const char* path, const TilingTable& t) {
@@ -1415,7 +1419,7 @@ extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, in
     }
     b->members.push_back(solves[i]);
     b->stop.push_back(-1);
-    b->m_chunk.push_back(64);
+    b->m_chunk.push_back(128);
     b->m_w4.push_back(1);
     fast = fast && solves[i]->use2 && solves[i]->ty2 == 32 && solves[i]->prm.d1 == 2 &&
            solves[i]->dtype == solves[0]->dtype && solves[i]->nghost == 0;
@@ -1434,6 +1438,9 @@ extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, in
   if (!e && fast) e = ctx_alloc(ctx, reinterpret_cast<void**>(&b->d_mons), sizeof(BatchMon) * n);
   if (!e && fast) e = ctx_alloc(ctx, reinterpret_cast<void**>(&b->d_tickets), 4 * sizeof(unsigned));
   if (!e && fast) e = cudaMemsetAsync(b->d_tickets, 0, 4 * sizeof(unsigned), ctx->stream);
+  if (!e && fast)
+    e = ctx_alloc(ctx, reinterpret_cast<void**>(&b->d_sync), batch_sync_words(n) * sizeof(unsigned));
+  if (const char* ech = std::getenv("FSLBM_BATCH_CHAIN")) b->chain = std::max(1, std::atoi(ech));
   if (!e) e = cudaEventCreate(&b->ev0);
   if (!e) e = cudaEventCreate(&b->ev1);
   if (e) {
@@ -1469,31 +1476,38 @@ extern "C" int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int use_graph) {
   }
   if (int r = batch_upload(b)) return r;
   CUDA_TRY(cudaEventRecord(b->ev0, st));
-  int64_t left = nsteps;
-  if (use_graph && left >= 2) {
+  // chained launches of `chain` steps (one graph replay each when use_graph), then the rest in
+  // one more launch; every launch leaves the members on their launch-start buffer when it has an
+  // even step count, so the graph replays from the same descriptors
+  const int G = b->chain + (b->chain & 1);
+  int64_t left = nsteps, nlaunch = 0;
+  if (use_graph && left >= G) {
     if (!b->exec2) {
       cudaGraph_t graph;
       CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      cudaError_t e1 = batch_enqueue_one(b, 0, st);
-      cudaError_t e2 = e1 ? e1 : batch_enqueue_one(b, 1, st);
-      cudaError_t e3 = cudaStreamEndCapture(st, &graph);
-      if (e2 || e3)
+      cudaError_t e1 = batch_enqueue(b, G, st);
+      cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+      if (e1 || e2)
         return fslbm_set_error(FSLBM_ERR_CUDA, "batch_step: graph capture: %s",
-                               cudaGetErrorString(e2 ? e2 : e3));
-      cudaError_t e4 = cudaGraphInstantiate(&b->exec2, graph, 0);
+                               cudaGetErrorString(e1 ? e1 : e2));
+      cudaError_t e3 = cudaGraphInstantiate(&b->exec2, graph, 0);
       cudaGraphDestroy(graph);
-      if (e4) return fslbm_set_error(FSLBM_ERR_CUDA, "batch_step: graph instantiate: %s", cudaGetErrorString(e4));
+      if (e3) return fslbm_set_error(FSLBM_ERR_CUDA, "batch_step: graph instantiate: %s", cudaGetErrorString(e3));
     }
-    for (; left >= 2; left -= 2) CUDA_TRY(cudaGraphLaunch(b->exec2, st));
+    for (; left >= G; left -= G, ++nlaunch) CUDA_TRY(cudaGraphLaunch(b->exec2, st));
   }
-  int parity = 0;
-  for (; left > 0; --left, parity ^= 1) CUDA_TRY(batch_enqueue_one(b, parity, st));
+  for (; left >= G; left -= G, ++nlaunch) CUDA_TRY(batch_enqueue(b, G, st));
+  if (left > 0) {
+    CUDA_TRY(batch_enqueue(b, int(left), st));
+    ++nlaunch;
+  }
   CUDA_TRY(cudaEventRecord(b->ev1, st));
   for (size_t i = 0; i < b->members.size(); ++i) {
     fslbm_solve* s = b->members[i];
     s->steps += take[i];
     s->cur ^= int(take[i] & 1);
-    s->launches += 2 * take[i];  // counted per member: each batched launch serves all members
+    // counted per member: each chained launch serves all members
+    s->launches += std::min<int64_t>(nlaunch, (take[i] + G - 1) / G);
   }
   return FSLBM_OK;
 }
@@ -1548,8 +1562,8 @@ extern "C" int fslbm_batch_load_tiling(fslbm_batch* b, const char* path) {
   return FSLBM_OK;
 }
 
-// Times candidate tilings on the batch itself: first one tiling for all members (chunks 32, 64,
-// 128 planes, both warp shapes), then per size class, largest first, the neighbouring chunks and
+// Times candidate tilings on the batch itself: first one tiling for all members (chunks 64, 128,
+// 256 planes, both warp shapes), then per size class, largest first, the neighbouring chunks and
 // the other warp shape while the other classes keep theirs; a change is kept only when it is at
 // least 0.3 % faster (each timing is the better of two trials). The members' fields, step
 // counts, monitor logs and gauges are restored afterwards.
@@ -1612,7 +1626,7 @@ extern "C" int fslbm_batch_autotune(fslbm_batch* b, int trial_steps, const char*
   Tiling glob;
   glob.ms = 1e30;
   for (int w = 1; w >= 0 && !rc; --w)
-    for (int c : {32, 64, 128}) {
+    for (int c : {64, 128, 256}) {
       set(all, c, w);
       double ms = 0;
       if ((rc = trial(&ms))) break;

@@ -88,12 +88,15 @@ cudaError_t fill_batch_member(void* dst, const CUtensorMap* map_p, const CUtenso
                               const StepLaunch& a, void* state0, void* state1,
                               const double* gauge_slot, const long long* steps, long long stop_at,
                               int monitor_every, int cur0, int nchunks, int w16x4);
-// items: nitems (member, item of the member) pairs; tickets: two counters (per step parity)
-// that start at zero; the bookkeeping launch resets the one its step used.
-cudaError_t launch_batch_step(int dtype, const void* members, const int2* items, int nitems,
-                              int grid, int parity, int packed, unsigned* tickets, cudaStream_t st);
-cudaError_t launch_batch_monitor(const BatchMon* mons, int n, int parity_after, unsigned* tickets,
-                                 cudaStream_t st);
+// Advances every member `nsteps` steps (fewer for members that reach their stop) in one
+// persistent launch, preceded by a reset of the launch's counters. items: nitems (member, item
+// of the member) pairs, longest first; mons: per-member bookkeeping (step counter, monitor);
+// sync: batch_sync_words(nmembers) counters; err: the batch's error flag. Step s of the launch
+// reads buffer cur0 ^ (s & 1) of each member.
+size_t batch_sync_words(int nmembers);
+cudaError_t launch_batch_steps(int dtype, const void* members, const BatchMon* mons,
+                               const int2* items, int nitems, int nsteps, int grid, int packed,
+                               unsigned* sync, int nmembers, unsigned* err, cudaStream_t st);
 
 // Seeded Poiseuille start written into a pitched state (walls and pad columns zero).
 cudaError_t launch_init_poiseuille(int dtype, void* state, const uint8_t* mask, int planes, int lxp,

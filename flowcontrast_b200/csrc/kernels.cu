@@ -196,6 +196,8 @@ __device__ void block_sum(double (&v)[NV], double* sh /* NV * 32 */) {
 // ------------------------------------------------------------------------------------------
 // monitor (FSLBM.cu:632-666), FP64 sums, one block
 // ------------------------------------------------------------------------------------------
+// The state is read through L2 (ld.global.cg): in a chained batched launch other CTAs of the
+// same grid wrote it, and this SM's L1 may hold lines of an earlier read of the same buffer.
 template <class TS>
 __device__ void monitor_body(const MonitorLaunch& a, double* sh) {
   using TA = typename ArithOf<TS>::type;
@@ -205,8 +207,8 @@ __device__ void monitor_body(const MonitorLaunch& a, double* sh) {
   double v[3] = {0, 0, 0};   // sum w, sum p, sum (p - pin) over non-wall cells of plane z=0
   for (int j = threadIdx.x; j < a.lxp * a.ly; j += blockDim.x) {
     if (a.mask[j] != 0) continue;           // walls hold zero; periodic images are not counted
-    const TA p = TA(st[j]);
-    v[0] += to_d(st[3 * FS + j]);
+    const TA p = TA(__ldcg(st + j));
+    v[0] += to_d(__ldcg(st + 3 * FS + j));
     v[1] += double(p);
     v[2] += double(TA(p - pin));            // the outlet buffer copy's p
   }
@@ -217,7 +219,7 @@ __device__ void monitor_body(const MonitorLaunch& a, double* sh) {
     r.step = a.counters->steps;
     r.q1 = q1; r.q2 = q1; r.p1 = p1; r.p2 = p2;
     r.f = (p1 - p2) / q1 / q1 / 3.0 * 4.0 * a.radius / double(a.L);
-    r.sample = to_d(st[3 * FS + (size_t(a.sz) * a.ly + a.sy) * a.lxp + a.sx]);
+    r.sample = to_d(__ldcg(st + 3 * FS + (size_t(a.sz) * a.ly + a.sy) * a.lxp + a.sx));
     r.re = 2.0 * a.radius * q1 / a.nu;
     const long long idx = a.counters->records;
     a.log[idx % a.log_cap] = r;
@@ -232,34 +234,155 @@ __global__ void monitor_kernel(MonitorLaunch a) {
   monitor_body<TS>(a, sh);
 }
 
-// Batched bookkeeping after a batched step: block i advances member i's step counter and, when
-// the member is due, writes its monitor record and the gauge of its next step.
-__global__ void batch_monitor_kernel(const BatchMon* mons, int parity_after, unsigned* tickets) {
-  __shared__ double sh[3 * 32];
-  __shared__ int due;
-  const BatchMon& b = mons[blockIdx.x];
+// ------------------------------------------------------------------------------------------
+// batched ensemble: chained steps in one persistent launch
+// ------------------------------------------------------------------------------------------
+// One member of a batched ensemble: its tensor maps for both state buffers, its step geometry
+// and constants, and where its step count stops.
+struct alignas(64) BatchMember {
+  CUtensorMap map_p[2], map_u[2];
+  Step2Geom g;                 // g.out is replaced by the buffer the step writes
+  StepConst<float> k;
+  void* state[2];
+  const double* gauge_slot;    // the member's monitor p2, applied on the step after a monitor
+  const long long* steps;      // the member's device step counter
+  long long stop_at;           // the member is not stepped once its counter reaches this
+  int w16x4;                   // warp shape of the member's items (16 x 4 instead of 32 x 2)
+  int monitor_every;
+  int cur0;                    // input buffer at the launch's first step
+};
+
+// Bookkeeping of one member after one of its steps, by all threads of the CTA that completed
+// the step's last item: the step counter advances (unless the member had reached its stop) and,
+// when due, the monitor record and the gauge of the member's next step are written. Not inlined:
+// it runs once per member and step, and inlined its reduction would share (and raise) the
+// register allocation of the march.
+__device__ __forceinline__ void batch_book(const BatchMon& b, int parity_after, double* sh, int* due) {
   if (threadIdx.x == 0) {
-    if (blockIdx.x == 0) tickets[parity_after ^ 1] = 0u;   // the step that just ran is complete
-    const long long s0 = b.mon.counters->steps;
-    due = 0;
+    const long long s0 = __ldcg(&b.mon.counters->steps);
+    *due = 0;
     if (s0 < b.stop_at) {
       const long long s = s0 + 1;
       b.mon.counters->steps = s;
-      due = b.monitor_every > 0 && s % b.monitor_every == 0;
+      *due = b.monitor_every > 0 && s % b.monitor_every == 0;
     }
   }
   __syncthreads();
-  if (!due) return;
-  MonitorLaunch a = b.mon;
-  a.state = b.state[b.cur0 ^ parity_after];
-  if (a.dtype == FSLBM_F16) monitor_body<__half>(a, sh);
-  else monitor_body<float>(a, sh);
+  if (*due) {
+    MonitorLaunch a = b.mon;
+    a.state = b.state[b.cur0 ^ parity_after];
+    if (a.dtype == FSLBM_F16) monitor_body<__half>(a, sh);
+    else monitor_body<float>(a, sh);
+  }
 }
 
-cudaError_t launch_batch_monitor(const BatchMon* mons, int n, int parity_after, unsigned* tickets,
-                                 cudaStream_t st) {
-  batch_monitor_kernel<<<n, 512, 0, st>>>(mons, parity_after, tickets);
-  return cudaGetLastError();
+// Thread 0, before an item of the member's step `step`: waits until the member's previous step
+// is complete and booked, then stages the item's geometry and constants in shared memory.
+// False when the wait gave up (error flag set). Not inlined, like the other per-item helpers
+// below: the march's register allocation stays its own.
+__device__ __forceinline__ bool batch_item_begin(const BatchMember& mb, int member, int step,
+                                              const unsigned* sync, unsigned* err, Step2Geom* s_g,
+                                              StepConst<float>* s_k, long long* s_done) {
+  if (step > 0 && !wait_geq_gpu(sync + 5 + 2 * member, unsigned(step), kWaitLimitNs)) {
+    atomicOr(err, 1u);
+    return false;
+  }
+  // the member's previous step was written by other CTAs through the generic proxy; this
+  // thread's TMA loads of it follow
+  fence_proxy_async_global();
+  const long long done = __ldcg(mb.steps);
+  *s_done = done;
+  const int cur = mb.cur0 ^ (step & 1);
+  Step2Geom g = mb.g;
+  g.out = mb.state[1 - cur];
+  g.step_counter = nullptr;
+  g.step_no = unsigned(done + 1);
+  g.gauge = (mb.monitor_every > 0 && done > 0 && done % mb.monitor_every == 0) ? mb.gauge_slot : nullptr;
+  *s_g = g;
+  *s_k = mb.k;
+  return true;
+}
+
+// Many pipes, `nsteps` steps each, in one persistent launch (nitems * nsteps < 2^32). Ticket t
+// is step t / nitems of item items[t % nitems] = (member, item of the member); within a step the
+// items are ordered longest first. Steps are chained per member instead of separated by
+// launches: before it marches an item of step s > 0, a CTA waits until the member's step s - 1
+// is complete and booked, so the members that finish a step early start the next one while the
+// last items of the step still run, and the SMs stay busy across step boundaries. A CTA waits
+// only on items that resident CTAs have already claimed (every ticket of step s precedes every
+// ticket of step s + 1), so the waits end. Counters (zeroed before the launch): sync[0] = next
+// ticket; per member m, sync[4 + 2m] = its items completed in this launch and sync[5 + 2m] =
+// its steps released.
+// A CTA counts its previous item when it claims the next one: after the claim's barrier every
+// thread's stores of that item precede thread 0's fence and its acq_rel count (cumulative over
+// the barrier). The CTA whose count completes a member's step books it (step counter, monitor)
+// and releases it before marching on. Counting there rather than right after the march keeps
+// the march free of register spills.
+template <int D1, int TY, bool PK, class TE>
+__global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
+    fslbm_step2_batch_kernel(const BatchMember* __restrict__ members,
+                             const BatchMon* __restrict__ mons, const int2* __restrict__ items,
+                             int nitems, int nsteps, unsigned* sync, unsigned* err) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ unsigned s_ticket;
+  __shared__ long long s_done;
+  __shared__ int s_go, s_book, s_due;
+  __shared__ double s_sh[3 * 32];
+  // the item's geometry and constants, read by the march from shared memory (the single-pipe
+  // kernel reads them from the parameter bank); kept in registers through the march they spill
+  __shared__ StepConst<float> s_k;
+  __shared__ Step2Geom s_g;
+  bool first = true;
+  unsigned prev = ~0u;             // the CTA's previous ticket, counted at the next claim
+  for (;;) {
+    if (threadIdx.x == 0) s_ticket = atomicAdd(&sync[0], 1u);
+    __syncthreads();               // every thread has finished the previous item
+    const unsigned t = s_ticket;
+    if (threadIdx.x == 0) {
+      s_book = -1;
+      if (prev != ~0u) {
+        __threadfence();
+        const int pm = items[prev % unsigned(nitems)].x;
+        const int ps = int(prev / unsigned(nitems));
+        const BatchMember& pb = members[pm];
+        const unsigned per_step = unsigned(pb.g.ntiles * pb.g.nchunks);
+        const unsigned c = atom_add_acq_rel_gpu(sync + 4 + 2 * pm, 1u) + 1u;
+        if (c == per_step * unsigned(ps + 1)) s_book = int(prev);
+      }
+    }
+    __syncthreads();               // every thread has read the ticket before the next claim
+    if (s_book >= 0) {             // the previous item completed its member's step: book, release
+      const unsigned pt = unsigned(s_book);
+      const int pm = items[pt % unsigned(nitems)].x;
+      const int ps = int(pt / unsigned(nitems));
+      batch_book(mons[pm], (ps & 1) ^ 1, s_sh, &s_due);
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) st_release_gpu(sync + 5 + 2 * pm, unsigned(ps + 1));
+    }
+    if (t >= unsigned(nitems) * unsigned(nsteps)) return;
+    const int step = int(t / unsigned(nitems));
+    const int2 it = items[t % unsigned(nitems)];
+    const BatchMember& mb = members[it.x];
+    if (threadIdx.x == 0)          // every thread has left the previous item (ticket barriers)
+      s_go = batch_item_begin(mb, it.x, step, sync, err, &s_g, &s_k, &s_done);
+    __syncthreads();
+    if (!s_go) return;
+    prev = t;
+    if (s_done < mb.stop_at) {
+      const int cur = mb.cur0 ^ (step & 1);
+      const int ntiles = mb.g.ntiles;
+      // the warp shape is a compile-time choice (a runtime one raises register pressure)
+      const bool ok = mb.w16x4 ? step2_march<D1, TY, PK, TE, true>(&mb.map_p[cur], &mb.map_u[cur], s_g,
+                                                                   s_k, it.y % ntiles, it.y / ntiles,
+                                                                   smem, !first)
+                               : step2_march<D1, TY, PK, TE, false>(&mb.map_p[cur], &mb.map_u[cur], s_g,
+                                                                    s_k, it.y % ntiles, it.y / ntiles,
+                                                                    smem, !first);
+      if (!ok) return;
+      first = false;
+    }
+  }
 }
 
 template <bool PK, class TE> static cudaError_t batch_prep() {
@@ -305,22 +428,29 @@ cudaError_t fill_batch_member(void* dst, const CUtensorMap* mp, const CUtensorMa
 }
 
 template <class TE>
-static void launch_batch_t(const BatchMember* mb, const int2* items, int nitems, int grid,
-                           int parity, int packed, unsigned* tickets, cudaStream_t st) {
+static void launch_batch_t(const BatchMember* mb, const BatchMon* mons, const int2* items,
+                           int nitems, int nsteps, int grid, int packed, unsigned* sync,
+                           unsigned* err, cudaStream_t st) {
   using Tl = Step2Tile<2, 32, TE>;
   if (packed)
     fslbm_step2_batch_kernel<2, 32, true, TE><<<grid, Tl::THREADS, Tl::SMEM_BYTES, st>>>(
-        mb, items, nitems, parity, tickets);
+        mb, mons, items, nitems, nsteps, sync, err);
   else
     fslbm_step2_batch_kernel<2, 32, false, TE><<<grid, Tl::THREADS, Tl::SMEM_BYTES, st>>>(
-        mb, items, nitems, parity, tickets);
+        mb, mons, items, nitems, nsteps, sync, err);
 }
 
-cudaError_t launch_batch_step(int dtype, const void* members, const int2* items, int nitems,
-                              int grid, int parity, int packed, unsigned* tickets, cudaStream_t st) {
+size_t batch_sync_words(int nmembers) { return 4 + 2 * size_t(nmembers); }
+
+cudaError_t launch_batch_steps(int dtype, const void* members, const BatchMon* mons,
+                               const int2* items, int nitems, int nsteps, int grid, int packed,
+                               unsigned* sync, int nmembers, unsigned* err, cudaStream_t st) {
+  if (nsteps < 1) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(sync, 0, batch_sync_words(nmembers) * sizeof(unsigned), st);
+  if (e) return e;
   const BatchMember* mb = reinterpret_cast<const BatchMember*>(members);
-  if (dtype == FSLBM_F32) launch_batch_t<float>(mb, items, nitems, grid, parity, packed, tickets, st);
-  else if (dtype == FSLBM_F16) launch_batch_t<__half>(mb, items, nitems, grid, parity, packed, tickets, st);
+  if (dtype == FSLBM_F32) launch_batch_t<float>(mb, mons, items, nitems, nsteps, grid, packed, sync, err, st);
+  else if (dtype == FSLBM_F16) launch_batch_t<__half>(mb, mons, items, nitems, nsteps, grid, packed, sync, err, st);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }

@@ -75,6 +75,42 @@ __device__ __forceinline__ uint32_t atom_add_acq_rel_cta(uint32_t* p, uint32_t v
   return old;
 }
 
+// ---- ordering between CTAs of one grid (gpu scope)
+// Counter add with acquire-release semantics at gpu scope. Returns the previous value.
+__device__ __forceinline__ uint32_t atom_add_acq_rel_gpu(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
+               : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Generic-proxy global accesses ordered before this point (including other CTAs' writes this
+// thread has acquired) are ordered before this thread's later async-proxy (TMA) accesses.
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+// Waits until *p >= target (acquire); false when `limit_ns` passed first.
+__device__ __forceinline__ bool wait_geq_gpu(const uint32_t* p, uint32_t target, uint64_t limit_ns) {
+  if (ld_acquire_gpu(p) >= target) return true;
+  const uint64_t t0 = global_timer_ns();
+  while (true) {
+    __nanosleep(128);
+    if (ld_acquire_gpu(p) >= target) return true;
+    if (global_timer_ns() - t0 > limit_ns) return false;
+  }
+}
+
 // 4-D tiled TMA load into this CTA's shared memory, completion counted on `bar`.
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar,
                                             int c0, int c1, int c2, int c3) {

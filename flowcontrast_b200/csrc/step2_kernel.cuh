@@ -8,11 +8,10 @@
 //  - a 32 x TY tile per CTA (512 threads for TY = 32, 16 warps per SM); p is staged with a
 //    one-cell halo, u,v,w with the corrector's 2*d1 halo, as two TMA boxes per plane into a
 //    window of 8 planes (output plane .. 3 planes ahead for d1 = 2);
-//  - no block-wide barrier in the march: per-slot "full" mbarriers count TMA completion, and
-//    each warp releases a slot after its last read of the plane in it, so warps drift within
-//    the window. The single-pipe kernel lets the last warp to release a slot refill it (no warp
-//    waits for a free slot); the batched kernel has thread 0 wait on per-slot "empty"
-//    mbarriers and refill;
+//  - no block-wide barrier in the march and no producer thread: per-slot "full" mbarriers count
+//    TMA completion, each warp releases a slot after its last read of the plane in it, and the
+//    last warp to release a slot refills it, so warps drift within the window and none waits
+//    for a free slot;
 //  - the streamwise corrector taps behind the output plane come from a 2*d1 register history
 //    of the thread's own columns, the taps ahead from the window;
 //  - grid = tiles x streamwise chunks in chunk-major order, so concurrent CTAs work at nearby
@@ -55,8 +54,8 @@ template <int D1, int TY, class TE = float> struct Step2Tile {
   static constexpr uint32_t TX_BYTES = uint32_t((SW * PH + 3 * UPLANE) * ES);
   static constexpr size_t RING_BYTES = size_t(S) * SLOT * ES;
   static constexpr size_t BAR_OFFSET = RING_BYTES;
-  // full and empty mbarriers per slot, then a release counter per slot
-  static constexpr size_t SMEM_BYTES = BAR_OFFSET + 2 * S * sizeof(uint64_t) + S * sizeof(uint32_t);
+  // a "full" mbarrier per slot, then a release counter per slot
+  static constexpr size_t SMEM_BYTES = BAR_OFFSET + S * sizeof(uint64_t) + S * sizeof(uint32_t);
   static_assert((PPLANE * ES) % 128 == 0 && (UPLANE * ES) % 16 == 0 && (SLOT * ES) % 128 == 0,
                 "TMA destinations must stay aligned");
   static_assert((HX * ES) % 16 == 0, "TMA box x start must be 16-byte aligned");
@@ -138,10 +137,6 @@ template <> struct Pair<false> {
   }
 };
 
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
 // Predictor brackets of one in-plane neighbour (cx, cy), see step_kernel.cuh:
 // P0 = q + a(3 + 4.5a), P1' = w(1 + 3a) (= P1/3), P2' = w^2 (= P2/4.5), a = cx u + cy v.
 template <bool PK, int CX, int CY>
@@ -175,25 +170,23 @@ __device__ __forceinline__ float2 qof(float2 P, float2 U, float2 V, float2 W) {
 // Marches one (tile, chunk) work item of one pipe: the step of every cell of the tile's columns
 // in the chunk's planes. `reinit` re-arms the CTA's mbarriers when the CTA has marched an item
 // before (persistent grids). Returns false when a bounded wait gave up (error flag set).
-// REFILL_LAST selects how freed window slots are refilled: by the last warp to release the slot
-// (no warp waits; +2 % on the single-pipe kernel) or by thread 0, which waits on the slot's empty
-// mbarrier (fewer live registers: the batched kernel, whose member state already presses on the
-// register budget, is 1 % faster this way).
-template <int D1, int TY, bool PK, class TE, bool W16X4 = false, bool REFILL_LAST = false>
+// Freed window slots are refilled by the last warp to release them (no warp waits for a free
+// slot); measured +2 % on the single pipe and +1.7 % on the batched ensemble against thread 0
+// waiting on per-slot "empty" mbarriers and refilling.
+template <int D1, int TY, bool PK, class TE, bool W16X4 = false>
 __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUtensorMap* tmap_uvw,
                                             const Step2Geom& g, const StepConst<float>& k,
                                             int tile, int chunk, unsigned char* smem, bool reinit) {
   using Tl = Step2Tile<D1, TY, TE>;
   using F = Pair<PK>;
   static_assert(D1 == 2, "the march prologue below is written for d1 = 2 (R = 4)");
-  constexpr int R = Tl::R, HX = Tl::HX, HY = Tl::HY, SW = Tl::SW, S = Tl::S, AH = Tl::AHEAD;
+  constexpr int R = Tl::R, HX = Tl::HX, HY = Tl::HY, SW = Tl::SW, S = Tl::S;
   constexpr int PPL = Tl::PPLANE, UPL = Tl::UPLANE, SLOT = Tl::SLOT;
 
   TE* ring = reinterpret_cast<TE*>(smem);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + Tl::BAR_OFFSET);
-  uint64_t* empty = full + S;     // per slot: one arrival per warp after its last read (thread 0 refills)
-  // per slot: warp releases, counted to elect the refilling warp (last-warp refill)
-  unsigned* released = reinterpret_cast<unsigned*>(empty + S);
+  // per slot: warp releases, counted to elect the refilling warp
+  unsigned* released = reinterpret_cast<unsigned*>(full + S);
 
   // Warp shape. Default: 32 columns x 2 rows (each half-warp reads one contiguous row).
   // W16X4: 16 columns (8 pairs) x 4 rows, so warps over wall skip at a finer grain, which pays
@@ -228,15 +221,9 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
   __syncthreads();   // a previous item (persistent grids) is fully consumed
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
-      if constexpr (REFILL_LAST) {
-        if (reinit) mbar_inval(&full[s]);
-        mbar_init(&full[s], 1);
-        released[s] = 0u;
-      } else {
-        if (reinit) { mbar_inval(&full[s]); mbar_inval(&empty[s]); }
-        mbar_init(&full[s], 1);
-        mbar_init(&empty[s], Tl::WARPS);
-      }
+      if (reinit) mbar_inval(&full[s]);
+      mbar_init(&full[s], 1);
+      released[s] = 0u;
     }
     mbar_init_fence();
   }
@@ -251,31 +238,16 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
     tma_load_4d(dst, tmap_p, &full[slot], org.x - HX, org.y - 1, zz, 0);
     tma_load_4d(dst + PPL, tmap_uvw, &full[slot], org.x - HX, org.y - HY, zz, 1);
   };
-  // Thread 0 loads the first planes: the whole ring (last-warp refill), or the output plane and
-  // AH planes ahead (thread-0 refill, which keeps the slots of planes m - R .. m - 1 for the
-  // corrector's taps behind).
-  int issued = -1;                                          // thread-0 refill: last plane issued
-  if (tid == 0) {
+  if (tid == 0) {                      // the whole ring up front
     prefetch_tensormap(tmap_p);
     prefetch_tensormap(tmap_uvw);
-    if constexpr (REFILL_LAST) {
-      for (int m = 0; m < S && m < niter; ++m) issue(m);
-    } else {
-      for (int m = 0; m <= AH && m < niter; ++m) { issue(m); issued = m; }
-    }
+    for (int m = 0; m < S && m < niter; ++m) issue(m);
   }
-  // failure path: let loads in flight land (bounded) before returning. With the last-warp refill
-  // any warp may have issued up to S planes ahead; otherwise thread 0 knows what it issued.
+  // failure path: any warp may have issued loads up to S planes ahead; let them land (bounded)
   auto drain = [&](int from) {
-    if constexpr (REFILL_LAST) {
-      if (lane == 0)
-        for (int q = from; q < niter && q < from + S; ++q)
-          mbar_wait_bounded(&full[q & (S - 1)], uint32_t((q / S) & 1), kWaitLimitNs / 8);
-    } else {
-      if (tid == 0)
-        for (int q = from; q <= issued; ++q)
-          mbar_wait_bounded(&full[q & (S - 1)], uint32_t((q / S) & 1), kWaitLimitNs / 8);
-    }
+    if (lane == 0)
+      for (int q = from; q < niter && q < from + S; ++q)
+        mbar_wait_bounded(&full[q & (S - 1)], uint32_t((q / S) & 1), kWaitLimitNs / 8);
   };
   // wait for march plane m; false after flagging a failure (the caller returns)
   auto arrive_wait = [&](int m) -> bool {
@@ -284,39 +256,21 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
     drain(m + 1);
     return false;
   };
-  // Plane m - R leaves the window and its slot takes plane m - R + S (= m + AH + 1).
-  // Last-warp refill: __syncwarp orders the warp's shared loads before lane 0's acq_rel add to the
-  // slot's counter; the warp whose add completes the count has acquired every warp's loads and
-  // orders them before its TMA write with a proxy fence. A slot's next cycle starts only after
-  // its refill lands, which needs all WARPS releases of this cycle, so the count is a multiple
-  // of WARPS exactly when a cycle is complete.
-  // Thread-0 refill: each warp arrives on the slot's empty mbarrier (release semantics) and
-  // thread 0 waits on it (acquire) before the proxy fence and the TMA.
+  // Plane m - R leaves the window and its slot takes plane m - R + S (= m + AHEAD + 1).
+  // __syncwarp orders the warp's shared loads before lane 0's acq_rel add to the slot's counter;
+  // the warp whose add completes the count has acquired every warp's loads and orders them
+  // before its TMA write with a proxy fence. A slot's next cycle starts only after its refill
+  // lands, which needs all WARPS releases of this cycle, so the count is a multiple of WARPS
+  // exactly when a cycle is complete.
   auto release_produce = [&](int m) -> bool {
     __syncwarp();
-    if constexpr (REFILL_LAST) {
-      if (m >= R && lane == 0) {
-        const int slot = (m - R) & (S - 1);
-        const unsigned seen = atom_add_acq_rel_cta(&released[slot], 1u) + 1u;
-        const int mn = m - R + S;
-        if (seen % unsigned(Tl::WARPS) == 0u && mn < niter) {
-          fence_proxy_async_smem();
-          issue(mn);
-        }
-      }
-    } else {
-      if (m >= R && lane == 0) mbar_arrive(&empty[(m - R) & (S - 1)]);
-      if (tid == 0 && m + AH + 1 < niter) {
-        const int mn = m + AH + 1;
-        if (mn >= S &&
-            !mbar_wait_bounded(&empty[mn & (S - 1)], uint32_t(((mn - S) / S) & 1), kWaitLimitNs)) {
-          atomicOr(g.err, 1u);
-          drain(m + 1);
-          return false;
-        }
+    if (m >= R && lane == 0) {
+      const int slot = (m - R) & (S - 1);
+      const unsigned seen = atom_add_acq_rel_cta(&released[slot], 1u) + 1u;
+      const int mn = m - R + S;
+      if (seen % unsigned(Tl::WARPS) == 0u && mn < niter) {
         fence_proxy_async_smem();
         issue(mn);
-        issued = mn;
       }
     }
     return true;
@@ -328,7 +282,9 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
     return true;
   }
 
-  const float gauge = g.gauge ? float(*g.gauge) : 0.0f;
+  // the gauge may have been written by another CTA of the same (chained batched) launch: read
+  // it from L2, not from a possibly stale L1 line
+  const float gauge = g.gauge ? float(__ldcg(g.gauge)) : 0.0f;
   const size_t FS = size_t(g.lxp) * g.ly * g.L;
   const TE* obase = reinterpret_cast<const TE*>(g.out);
   const uint32_t seed = hash32(g.step_no * 0x9e3779b9u + 0x632be5abu);
@@ -557,72 +513,8 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
                        const StepConst<float> k) {
   extern __shared__ __align__(128) unsigned char smem[];
   if (threadIdx.x == 0 && blockIdx.x == 0 && g.step_counter) *g.step_counter += 1;
-  step2_march<D1, TY, PK, TE, false, true>(&tmap_p, &tmap_uvw, g, k, blockIdx.x % g.ntiles,
+  step2_march<D1, TY, PK, TE>(&tmap_p, &tmap_uvw, g, k, blockIdx.x % g.ntiles,
                           blockIdx.x / g.ntiles, smem, false);
-}
-
-// One member of a batched ensemble: its tensor maps for both state buffers, its step geometry
-// and constants, and where its step count stops.
-struct alignas(64) BatchMember {
-  CUtensorMap map_p[2], map_u[2];
-  Step2Geom g;                 // g.out is replaced by the buffer the step writes
-  StepConst<float> k;
-  void* state[2];
-  const double* gauge_slot;    // the member's monitor p2, applied on the step after a monitor
-  const long long* steps;      // the member's device step counter
-  long long stop_at;           // the member is not stepped once its counter reaches this
-  int w16x4;                   // warp shape of the member's items (16 x 4 instead of 32 x 2)
-  int monitor_every;
-  int cur0;                    // input buffer at batch parity 0
-};
-
-// Many pipes, one step each: a persistent grid claims work items from a ticket counter (one
-// per step parity; the bookkeeping launch after the step resets it). items[t] = (member, item
-// of that member), longest items first, so uneven members balance across the SMs.
-template <int D1, int TY, bool PK, class TE>
-__global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
-    fslbm_step2_batch_kernel(const BatchMember* __restrict__ members, const int2* __restrict__ items,
-                             int nitems, int parity, unsigned* tickets) {
-  extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ int s_item;
-  // the item's geometry and constants, read by the march from shared memory (the single-pipe
-  // kernel reads them from the parameter bank); kept in registers through the march they spill
-  __shared__ StepConst<float> s_k;
-  __shared__ Step2Geom s_g;
-  bool first = true;
-  for (;;) {
-    if (threadIdx.x == 0) s_item = int(atomicAdd(&tickets[parity], 1u));
-    __syncthreads();
-    const int t = s_item;
-    __syncthreads();               // every thread has read the ticket before the next claim
-    if (t >= nitems) return;
-    const int2 it = items[t];
-    const BatchMember& mb = members[it.x];
-    const long long done = *mb.steps;
-    if (done >= mb.stop_at) continue;
-    const int cur = mb.cur0 ^ parity;
-    const int ntiles = mb.g.ntiles;
-    if (threadIdx.x == 0) {            // every thread has left the previous item (ticket barriers)
-      Step2Geom g = mb.g;
-      g.out = mb.state[1 - cur];
-      g.step_counter = nullptr;
-      g.step_no = unsigned(done + 1);
-      g.gauge = (mb.monitor_every > 0 && done > 0 && done % mb.monitor_every == 0) ? mb.gauge_slot
-                                                                                : nullptr;
-      s_g = g;
-      s_k = mb.k;
-    }
-    __syncthreads();
-    // the warp shape is a compile-time choice (a runtime one raises register pressure)
-    const bool ok = mb.w16x4 ? step2_march<D1, TY, PK, TE, true>(&mb.map_p[cur], &mb.map_u[cur], s_g,
-                                                                 s_k, it.y % ntiles, it.y / ntiles,
-                                                                 smem, !first)
-                             : step2_march<D1, TY, PK, TE, false>(&mb.map_p[cur], &mb.map_u[cur], s_g,
-                                                                  s_k, it.y % ntiles, it.y / ntiles,
-                                                                  smem, !first);
-    if (!ok) return;
-    first = false;
-  }
 }
 
 }  // namespace fslbm

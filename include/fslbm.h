@@ -196,13 +196,15 @@ int fslbm_profile_sample(fslbm_solve* s);
 int fslbm_profile_get(fslbm_solve* s, double* sums, int64_t* nsamples);
 int fslbm_profile_reset(fslbm_solve* s);
 
-/* ---- batched ensemble: many solves advanced by one persistent launch per step group ---- */
+/* ---- batched ensemble: many solves advanced together by persistent launches ---- */
 int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, int n, fslbm_batch** out);
 int fslbm_batch_destroy(fslbm_batch* b);
-/* Advances every member nsteps steps, asynchronously. When every member is FP32 with d1 = 2, a
- * time step of the whole ensemble is one persistent launch over all members' (tile, chunk) work
- * items plus one bookkeeping launch (step counters, monitors, gauges); with use_graph two such
- * steps are replayed from a captured CUDA graph. Other members step one after another. */
+/* Advances every member nsteps steps, asynchronously. When every member is FP32 or FP16 storage
+ * with d1 = 2, up to 16 time steps of the whole ensemble (FSLBM_BATCH_CHAIN) run in one
+ * persistent launch over all members' (tile, chunk) work items, each member's next step
+ * starting as soon as its previous step is complete (step counters, monitors and gauges are
+ * kept inside the launch); with use_graph each such launch is replayed from a captured CUDA
+ * graph. Other members step one after another. */
 int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int use_graph);
 int fslbm_batch_sync(fslbm_batch* b);
 /* Device time of the last fslbm_batch_step call (valid after fslbm_batch_sync). */
