@@ -136,13 +136,13 @@ class ClockSampler:
                 "samples": len(inside)}
 
 
-def read_traffic():
-    """DRAM bytes per step-kernel launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "fslbm_step2_f32_512x128x128.md")
+def read_traffic(summary="fslbm_step2_f32_512x128x128.md", key="dram_bytes_per_launch_full_size"):
+    """DRAM bytes (read + write) from a committed ncu summary under profiles/, if present."""
+    path = os.path.join(ROOT, "profiles", summary)
     if not os.path.exists(path):
         return None
     for line in open(path):
-        if line.strip().startswith("dram_bytes_per_launch_full_size:"):
+        if line.strip().startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1].split()[0])
             except ValueError:
@@ -495,7 +495,10 @@ def run_ensemble(args):
             "autotune": {"seconds": t_tune, "classes": len(table), "trial_steps": 20},
             "batch_equals_plain_bitwise": bool(same),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         "traffic": read_traffic("fslbm_step2_batch_kernel_ensemble64.md",
+                                                 "dram_bytes_per_step_full_size"),
+                         "traffic_unit": "bytes per ensemble step (one step of the chained launch)",
                          "peak_source": f"{peak_kind} hbm_gbs",
                          "kernel": "fslbm_step2_batch_kernel<2,32,scalar,float> (chained steps)"},
             "e2e": {"value": cells * args.steps / e2e_s / 1e6, "unit": "MLUPS",
@@ -573,6 +576,22 @@ def run_served(args):
                        "equals_alone": bool(np.array_equal(g, out["same"])),
                        "rel_l2_u_vs_f64": float(np.linalg.norm(g[1:] - out["f64"][1:]) /
                                                 np.linalg.norm(out["f64"][1:]))})
+    # the plain method on the same stream: a seeded sample of the requests run one at a time
+    # (each its full step count), aggregate MLUPS = sample work / sample device time
+    rng = np.random.default_rng(7)
+    sample = sorted(rng.choice(len(reqs), size=min(32, len(reqs)), replace=False).tolist())
+    alone_work = alone_ms = 0.0
+    for k in sample:
+        sp = reqs[k]
+        s = fb.Solve(ctx, sp.domain(fb), sp.params(fb), sp.dtype)
+        s.init_poiseuille(2 * wl.U_BULK, noise=1e-3, modes=4, mode_amp=0.05, seed=sp.seed)
+        s.set_timing(True)
+        s.step(sp.steps)
+        s.sync()
+        alone_ms += s.info()["last_step_ms"]
+        alone_work += sp.cells * sp.steps
+        s.close()
+    plain_alone = alone_work / (alone_ms * 1e-3) / 1e6
     ctx.close()
     srv.close()
     line = {"metric": "aggregate MLUPS and p50/p95/p99 latency, served solves", "value": work / span / 1e6,
@@ -590,7 +609,11 @@ def run_served(args):
             "rounds": st["rounds"] - base["rounds"], "peak_device_bytes": st["bytes_peak"],
             "worker_seconds": {k: st[k] - base[k] for k in
                                ("t_admit", "t_regroup", "t_launch", "t_wait", "t_retire")},
-            "checks": checks, "clocks": clocks}
+            "checks": checks, "clocks": clocks,
+            "plain_one_at_a_time_mlups": plain_alone,
+            "plain_sample": f"{len(sample)} requests of the stream (seeded), each stepped alone on "
+                            "the plain path for its full step count, device time",
+            "speedup_vs_plain": work / span / 1e6 / plain_alone}
     print(json.dumps(line), flush=True)
     return 0
 
