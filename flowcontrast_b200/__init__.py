@@ -138,6 +138,7 @@ def lib():
             "fslbm_last_error": ([ctypes.c_char_p, ctypes.c_size_t], _i),
             "fslbm_ctx_create": ([_i, ctypes.POINTER(_vp)], _i),
             "fslbm_ctx_destroy": ([_vp], _i),
+            "fslbm_selftest_waits": ([_vp, ctypes.c_double, ctypes.POINTER(ctypes.c_uint)], _i),
             "fslbm_solve_create": ([_vp, ctypes.POINTER(Domain), ctypes.POINTER(Params), _i,
                                     ctypes.POINTER(_vp)], _i),
             "fslbm_solve_destroy": ([_vp], _i),
@@ -310,6 +311,13 @@ class Context:
         if self.handle:
             _check(lib().fslbm_ctx_destroy(self.handle))
             self.handle = None
+
+    def selftest_waits(self, limit_ms=2.0):
+        """Runs the device-side bounded waits against conditions nothing satisfies
+        (fslbm_selftest_waits); returns (status code, bits of the waits that gave up)."""
+        bits = ctypes.c_uint(0)
+        rc = lib().fslbm_selftest_waits(self.handle, float(limit_ms), ctypes.byref(bits))
+        return rc, bits.value
 
     def __enter__(self):
         return self

@@ -132,6 +132,26 @@ extern "C" int fslbm_ctx_destroy(fslbm_ctx* c) {
   return FSLBM_OK;
 }
 
+// Self-test of the device-side bounded waits (no reference counterpart): both give up after
+// limit_ms, the kernel returns, and the error is reported like any other gave-up wait.
+extern "C" int fslbm_selftest_waits(fslbm_ctx* c, double limit_ms, unsigned* gave_up) {
+  if (!c || !gave_up || !(limit_ms > 0.0) || limit_ms > 10000.0)
+    return fslbm_set_error(FSLBM_ERR_ARG, "selftest_waits: bad argument");
+  CUDA_TRY(cudaSetDevice(c->device));
+  unsigned* d = nullptr;                      // [0] the counter nobody sets, [1] error bits
+  CUDA_TRY(ctx_alloc(c, reinterpret_cast<void**>(&d), 2 * sizeof(unsigned)));
+  cudaError_t e = cudaMemsetAsync(d, 0, 2 * sizeof(unsigned), c->stream);
+  if (!e) e = launch_wait_selftest(d, static_cast<unsigned long long>(limit_ms * 1e6), d + 1, c->stream);
+  unsigned err = 0;
+  if (!e) e = cudaMemcpyAsync(&err, d + 1, sizeof err, cudaMemcpyDeviceToHost, c->stream);
+  ctx_free(c, d);
+  if (!e) e = cudaStreamSynchronize(c->stream);
+  if (e) return fslbm_set_error(FSLBM_ERR_CUDA, "selftest_waits: %s", cudaGetErrorString(e));
+  *gave_up = err;
+  if (err) return fslbm_set_error(FSLBM_ERR_TIMEOUT, "selftest_waits: bounded device waits gave up (bits %u)", err);
+  return FSLBM_OK;
+}
+
 // ------------------------------------------------------------------------------------------
 // tensor-map encoding through the driver entry point (no link-time libcuda dependency)
 // ------------------------------------------------------------------------------------------

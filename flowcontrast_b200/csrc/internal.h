@@ -72,6 +72,10 @@ struct MonitorLaunch {
   DevCounters* counters;
 };
 cudaError_t launch_monitor(const MonitorLaunch& a, cudaStream_t st);
+// The bounded waits against conditions nothing satisfies (counter stays 0): err bit 0 = the
+// counter wait gave up, bit 1 = the mbarrier wait gave up.
+cudaError_t launch_wait_selftest(const unsigned* counter, unsigned long long limit_ns, unsigned* err,
+                                 cudaStream_t st);
 
 // ---- batched ensemble (FP32 column-pair kernel, d1 = 2, tile height 32)
 struct BatchMon {

@@ -791,4 +791,28 @@ cudaError_t launch_gather_plane(int dtype, const void* state, int lx, int lxp, i
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------------------------------
+// self-test of the bounded device waits
+// ------------------------------------------------------------------------------------------
+// Runs the two bounded waits the kernels rely on against conditions nothing will satisfy: the
+// gpu-scope counter wait of the chained batched launch (on a counter that stays 0) and the
+// mbarrier phase wait of the march (on a barrier nobody arrives at; no copy is issued, so
+// nothing is in flight when it gives up). err bit 0 / bit 1 record that each gave up.
+__global__ void wait_selftest_kernel(const unsigned* counter, unsigned long long limit_ns,
+                                     unsigned* err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x != 0) return;
+  if (!wait_geq_gpu(counter, 1u, limit_ns)) atomicOr(err, 1u);
+  mbar_init(&bar, 1);
+  mbar_init_fence();
+  if (!mbar_wait_bounded(&bar, 0u, limit_ns)) atomicOr(err, 2u);
+  mbar_inval(&bar);
+}
+
+cudaError_t launch_wait_selftest(const unsigned* counter, unsigned long long limit_ns, unsigned* err,
+                                 cudaStream_t st) {
+  wait_selftest_kernel<<<1, 32, 0, st>>>(counter, limit_ns, err);
+  return cudaGetLastError();
+}
+
 }  // namespace fslbm

@@ -121,6 +121,12 @@ int fslbm_ctx_create(int device, fslbm_ctx** out);
    pool are released when the last of the context, its solves and its batches is destroyed
    (any order is safe). */
 int fslbm_ctx_destroy(fslbm_ctx* ctx);
+/* Self-test of the device-side bounded waits the kernels use (no reference counterpart): a
+   gpu-scope counter wait and an mbarrier phase wait, each on a condition nothing satisfies, with
+   a limit of limit_ms (0 < limit_ms <= 10000). Both give up and return; *gave_up gets one bit
+   per wait (3 = both) and the call returns FSLBM_ERR_TIMEOUT, the code a kernel's gave-up wait
+   produces. The context stays usable. */
+int fslbm_selftest_waits(fslbm_ctx* ctx, double limit_ms, unsigned* gave_up);
 
 /* ---- solve (replaces main's set-up and time loop, FSLBM.cu:489-905) ---- */
 int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const fslbm_params* prm,

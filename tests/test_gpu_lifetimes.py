@@ -36,3 +36,24 @@ def test_context_destroyed_before_its_solves(built):
     assert np.array_equal(b.get_fields(np.float32), want)
     batch.close()
     b.close()                        # the last reference: the context is released here
+
+
+def test_bounded_device_waits_give_up_and_report(built, ctx):
+    """The kernels' bounded waits (a gpu-scope counter wait of the chained batched launch, an
+    mbarrier phase wait of the march) run against conditions nothing satisfies: both give up
+    after the limit, the kernel returns, the host reads FSLBM_ERR_TIMEOUT, and the context keeps
+    working (a solve afterwards steps normally)."""
+    import time
+    fb = built
+    t0 = time.perf_counter()
+    rc, bits = ctx.selftest_waits(limit_ms=5.0)
+    dt = time.perf_counter() - t0
+    assert rc == -6 and bits == 3, (rc, bits)
+    assert dt < 5.0
+    s = small_solve(fb, ctx)
+    s.step(4)
+    s.sync()
+    assert np.isfinite(s.get_fields(np.float32)).all()
+    s.close()
+    with pytest.raises(fb.FslbmError):
+        fb._check(fb.lib().fslbm_selftest_waits(ctx.handle, -1.0, None))
