@@ -1499,7 +1499,10 @@ extern "C" int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int use_graph) {
   // chained launches of `chain` steps (one graph replay each when use_graph), then the rest in
   // one more launch; every launch leaves the members on their launch-start buffer when it has an
   // even step count, so the graph replays from the same descriptors
-  const int G = b->chain + (b->chain & 1);
+  // steps per launch: even (the graph replays from the same buffers) and few enough that the
+  // launch's 32-bit ticket count nitems * steps stays below 2^31
+  const int64_t cap = std::max<int64_t>(2, (int64_t(INT_MAX) / std::max(1, b->nitems)) & ~int64_t(1));
+  const int G = int(std::min<int64_t>(b->chain + (b->chain & 1), cap));
   int64_t left = nsteps, nlaunch = 0;
   if (use_graph && left >= G) {
     if (!b->exec2) {
@@ -1517,7 +1520,7 @@ extern "C" int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int use_graph) {
     for (; left >= G; left -= G, ++nlaunch) CUDA_TRY(cudaGraphLaunch(b->exec2, st));
   }
   for (; left >= G; left -= G, ++nlaunch) CUDA_TRY(batch_enqueue(b, G, st));
-  if (left > 0) {
+  if (left > 0) {                  // left < G
     CUDA_TRY(batch_enqueue(b, int(left), st));
     ++nlaunch;
   }
