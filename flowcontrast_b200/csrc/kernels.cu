@@ -254,9 +254,8 @@ struct alignas(64) BatchMember {
 
 // Bookkeeping of one member after one of its steps, by all threads of the CTA that completed
 // the step's last item: the step counter advances (unless the member had reached its stop) and,
-// when due, the monitor record and the gauge of the member's next step are written. Not inlined:
-// it runs once per member and step, and inlined its reduction would share (and raise) the
-// register allocation of the march.
+// when due, the monitor record and the gauge of the member's next step are written. Inlined: any
+// call in the batched kernel makes its march spill registers (the call ABI).
 __device__ __forceinline__ void batch_book(const BatchMon& b, int parity_after, double* sh, int* due) {
   if (threadIdx.x == 0) {
     const long long s0 = __ldcg(&b.mon.counters->steps);
@@ -278,8 +277,7 @@ __device__ __forceinline__ void batch_book(const BatchMon& b, int parity_after, 
 
 // Thread 0, before an item of the member's step `step`: waits until the member's previous step
 // is complete and booked, then stages the item's geometry and constants in shared memory.
-// False when the wait gave up (error flag set). Not inlined, like the other per-item helpers
-// below: the march's register allocation stays its own.
+// False when the wait gave up (error flag set). Inlined for the same reason as batch_book.
 __device__ __forceinline__ bool batch_item_begin(const BatchMember& mb, int member, int step,
                                               const unsigned* sync, unsigned* err, Step2Geom* s_g,
                                               StepConst<float>* s_k, long long* s_done) {
