@@ -1223,6 +1223,7 @@ struct fslbm_batch {
   std::vector<unsigned char> h_members;
   std::vector<BatchMon> h_mons;
   std::vector<int2> h_items;
+  std::vector<int2> item_shape;    // per member: (tiles, chunks) the item table was built for
   int nitems = 0, grid = 0, packed = 1;
   // per member tiling: streamwise planes per work item and warp shape (16 x 4 or 32 x 2),
   // from the tuning table by size class, else 128 (FSLBM_BATCH_CHUNK) and 16 x 4
@@ -1270,10 +1271,27 @@ static int batch_upload(fslbm_batch* b) {
   cudaStream_t st = b->ctx->stream;
   b->h_members.assign(mbytes * n, 0);
   b->h_mons.resize(n);
+  // the batched kernel counts a member's step complete after ntiles * nchunks items, so the
+  // item table must match every member as it is now: a member reconfigured since the table was
+  // built (fslbm_solve_set_params) forces a rebuild, and one that no longer fits the kernel
+  // (stride, corrector order or storage type changed) is refused
+  for (int i = 0; i < n; ++i) {
+    const fslbm_solve* s = b->members[i];
+    if (!(s->use2 && s->ty2 == 32 && s->prm.d1 == 2 && s->dtype == b->members[0]->dtype && s->nghost == 0))
+      return fslbm_set_error(FSLBM_ERR_STATE, "batch_step: member %d was reconfigured and no longer "
+                             "fits the batched kernel; create a new batch", i);
+  }
+  auto eff_chunk = [&](int i) { return std::max(4 * b->members[i]->prm.d1, b->m_chunk[i] / b->shrink); };
+  if (!b->h_items.empty() && b->item_shape.size() == size_t(n))
+    for (int i = 0; i < n; ++i)
+      if (b->item_shape[i].x != b->members[i]->ntiles ||
+          b->item_shape[i].y != member_chunks(b->members[i], eff_chunk(i))) {
+        b->h_items.clear();
+        break;
+      }
   const bool build_items = b->h_items.empty();
   struct Item { int64_t cost; int2 it; };
   std::vector<Item> items;
-  auto eff_chunk = [&](int i) { return std::max(4 * b->members[i]->prm.d1, b->m_chunk[i] / b->shrink); };
   if (build_items) {
     // shorter chunks while there are fewer than two items per SM (few or small members)
     auto count = [&]() {
@@ -1297,6 +1315,10 @@ static int batch_upload(fslbm_batch* b) {
     CUDA_TRY(fill_batch_member(b->h_members.data() + mbytes * i, s->maps2p, s->maps2u, a,
                                s->state[0], s->state[1], s->d_gauge, &s->d_counters->steps,
                                stop_at, s->prm.monitor_every, s->cur, nch, b->m_w4[i]));
+    if (build_items) {
+      if (i == 0) b->item_shape.assign(n, make_int2(0, 0));
+      b->item_shape[i] = make_int2(s->ntiles, nch);
+    }
     if (build_items)
       for (int c = 0; c < nch; ++c) {
         const int nout = int((long long)s->L * (c + 1) / nch - (long long)s->L * c / nch);

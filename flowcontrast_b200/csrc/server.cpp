@@ -43,6 +43,7 @@ using ReqPtr = std::shared_ptr<Request>;
 
 struct Group {
   int dtype = 0;
+  std::vector<int64_t> ids;       // the members' request ids: the group's identity
   std::vector<fslbm_solve*> members;
   std::vector<int64_t> stops;     // each member's total step count
   fslbm_batch* batch = nullptr;
@@ -182,12 +183,16 @@ int regroup(fslbm_server* S) {
       next.back().dtype = r->req.dtype;
       it = next.end() - 1;
     }
+    it->ids.push_back(r->id);
     it->members.push_back(r->solve);
     it->stops.push_back(r->req.nsteps);
   }
+  // A batch is reused only for the same requests. Solve addresses are no identity: a solve
+  // created after another was destroyed can reuse its address, and a batch kept for it would
+  // step the new solve with the old one's work items and stop step.
   for (Group& g : next) {
     auto old = std::find_if(S->groups.begin(), S->groups.end(), [&](const Group& o) {
-      return o.dtype == g.dtype && o.members == g.members && o.batch;
+      return o.dtype == g.dtype && o.ids == g.ids && o.members == g.members && o.batch;
     });
     if (old != S->groups.end()) {
       g.batch = old->batch;

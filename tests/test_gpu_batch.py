@@ -142,3 +142,26 @@ def test_autotune_restores_state_and_keeps_results(built, ctx, tmp_path):
     b2.close()
     for s in members + again:
         s.close()
+
+
+def test_reconfigured_member_is_refused(built, ctx):
+    """The batched kernel counts a member's step complete after the member's own number of work
+    items; a member reconfigured after the batch was made (here to the order-6 corrector, which
+    the batched kernel does not run) is refused with FSLBM_ERR_STATE instead of being stepped
+    from a stale item table."""
+    fb = built
+    specs = member_specs(n=3, seed=31)
+    members = [make_member(fb, ctx, sp) for sp in specs]
+    b = fb.Batch(ctx, members)
+    b.step(4)
+    b.sync()
+    sp = specs[0]
+    members[0].set_params(fb.Params.make(tblend=0.5, pin=0.0, nu=sp["nu"], d1=2, delta=1,
+                                         blend=1.0, monitor_every=25,
+                                         force=(0.0, 0.0, -sp["g"]), fd_order=6))
+    with pytest.raises(fb.FslbmError) as e:
+        b.step(2)
+    assert e.value.code == -3
+    b.close()
+    for s in members:
+        s.close()

@@ -127,3 +127,39 @@ def test_served_rejects_and_fails(built):
         ok = srv.submit(dom, params(fb, R, 300.0), fb.F32, 10)
         assert srv.wait(rid, 60)["status"] == fb.REQ_FAILED
         assert srv.wait(ok, 60)["status"] == fb.REQ_DONE
+
+
+def test_many_admissions_after_retirements(built, ctx):
+    """Requests retire and new ones are admitted round after round (short step budgets, small
+    quantum, three waves). A new request's solve may land at the address of one that just
+    retired; the server must still build its batch for the new request (its own work items and
+    stop step): every request completes, and a spread of them equal the same request alone."""
+    fb = built
+    rng = np.random.default_rng(123)
+    waves = []
+    with fb.Server(0, quantum=7) as srv:
+        for wave in range(3):
+            ids = []
+            for k in range(8):
+                n = int(rng.integers(24, 60))
+                L = int(rng.integers(24, 80))
+                spec = (n, L, float(rng.uniform(60, 1500)), int(rng.integers(5, 40)),
+                        1 if k % 3 else 2, 1000 * wave + k)
+                dom, R = pipe(fb, n, L)
+                ids.append((srv.submit(dom, params(fb, R, spec[2]), spec[4], spec[3],
+                                       init_spec=dict(umax=0.2, noise=1e-3, modes=2,
+                                                      mode_amp=0.05, seed=spec[5])), spec))
+                time.sleep(0.003)
+            waves.append(ids)
+            time.sleep(0.01)
+        srv.drain(120)
+        st = srv.stats()
+        assert (st["completed"], st["failed"]) == (24, 0), (st["completed"], st["failed"])
+        for ids in waves:
+            for j, (rid, (n, L, re, steps, dt, seed)) in enumerate(ids):
+                res = srv.poll(rid)
+                assert res["status"] == fb.REQ_DONE and res["steps_done"] == steps
+                got = srv.release(rid)
+                if j % 3 == 0:
+                    want, _ = alone(fb, ctx, n, L, re, steps, dt, seed)
+                    assert np.array_equal(got, want), (n, L, dt, steps)
