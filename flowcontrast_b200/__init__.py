@@ -77,7 +77,11 @@ class Info(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_int64), ("max_resident", ctypes.c_int),
-                ("quantum", ctypes.c_int)]
+                ("quantum", ctypes.c_int), ("policy", ctypes.c_int),
+                ("round_cells", ctypes.c_int64)]
+
+
+SERVE_ALL, SERVE_LEAST_WORK = 0, 1
 
 
 class InitSpec(ctypes.Structure):
@@ -528,8 +532,12 @@ class Server:
     """Served solves with continuous batching (fslbm_server_*): its own context and worker
     thread on `device`. submit() returns a request id; results come back in FP32 arrays."""
 
-    def __init__(self, device=0, hbm_budget=0, max_resident=0, quantum=0):
-        cfg = ServerConfig(int(hbm_budget), int(max_resident), int(quantum))
+    def __init__(self, device=0, hbm_budget=0, max_resident=0, quantum=0, policy=SERVE_ALL,
+                 round_cells=0):
+        """policy SERVE_ALL advances every resident request each round; SERVE_LEAST_WORK the
+        ones with the least work left, up to round_cells box cells per round."""
+        cfg = ServerConfig(int(hbm_budget), int(max_resident), int(quantum), int(policy),
+                           int(round_cells))
         h = ctypes.c_void_p()
         _check(lib().fslbm_server_create(int(device), ctypes.byref(cfg), ctypes.byref(h)))
         self.handle = h

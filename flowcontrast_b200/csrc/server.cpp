@@ -37,6 +37,7 @@ struct Request {
   fslbm_solve* solve = nullptr;   // worker-owned while running
   int64_t left = 0;
   bool has_out = false;
+  bool in_round = false;          // worker-only: advanced by the current round
 };
 
 using ReqPtr = std::shared_ptr<Request>;
@@ -173,10 +174,28 @@ std::vector<ReqPtr> admit(fslbm_server* S, const std::vector<ReqPtr>& adm) {
   return started;
 }
 
-// Rebuilds the per-dtype groups whose membership changed.
-int regroup(fslbm_server* S) {
+// The resident requests a round advances: all of them, or (least-work policy) those with the
+// least work left, in that order, up to round_cells box cells and at least one.
+std::vector<ReqPtr> round_set(const fslbm_server* S) {
+  if (S->cfg.policy != FSLBM_SERVE_LEAST_WORK) return S->active;
+  std::vector<ReqPtr> order = S->active;
+  std::stable_sort(order.begin(), order.end(), [](const ReqPtr& a, const ReqPtr& b) {
+    return double(a->res.cells) * double(a->left) < double(b->res.cells) * double(b->left);
+  });
+  std::vector<ReqPtr> out;
+  int64_t cells = 0;
+  for (const ReqPtr& r : order) {
+    if (!out.empty() && cells + r->res.cells > S->cfg.round_cells) break;
+    out.push_back(r);
+    cells += r->res.cells;
+  }
+  return out;
+}
+
+// Rebuilds the per-dtype groups of the round's requests whose membership changed.
+int regroup(fslbm_server* S, const std::vector<ReqPtr>& round) {
   std::vector<Group> next;
-  for (const ReqPtr& r : S->active) {
+  for (const ReqPtr& r : round) {
     auto it = std::find_if(next.begin(), next.end(), [&](const Group& g) { return g.dtype == r->req.dtype; });
     if (it == next.end()) {
       next.push_back(Group{});
@@ -240,14 +259,16 @@ void run(fslbm_server* S) {
       continue;
     }
     const auto tg = Clock::now();
-    const int rg = regroup(S);
+    const std::vector<ReqPtr> round = round_set(S);
+    for (const ReqPtr& r : round) r->in_round = true;
+    const int rg = regroup(S, round);
     add_time(S, &fslbm_server_stats::t_regroup, tg);
     if (rg) {
       fail_active(S, rg);
       continue;
     }
     int64_t most = 0;
-    for (const ReqPtr& r : S->active) most = std::max(most, r->left);
+    for (const ReqPtr& r : round) most = std::max(most, r->left);
     const int64_t k = std::min<int64_t>(S->cfg.quantum, most);
     const auto tr = Clock::now();
     int rc = FSLBM_OK;
@@ -273,6 +294,11 @@ void run(fslbm_server* S) {
     std::vector<ReqPtr> still;
     const auto tt = Clock::now();
     for (const ReqPtr& r : S->active) {
+      if (!r->in_round) {            // waits for a later round
+        still.push_back(r);
+        continue;
+      }
+      r->in_round = false;
       const int64_t took = std::min(k, r->left);
       r->left -= took;
       {
@@ -301,6 +327,11 @@ extern "C" int fslbm_server_create(int device, const fslbm_server_config* cfg, f
   if (cfg) S->cfg = *cfg;
   if (S->cfg.hbm_budget <= 0) S->cfg.hbm_budget = int64_t(150e9);
   if (S->cfg.quantum <= 0) S->cfg.quantum = 50;
+  if (S->cfg.round_cells <= 0) S->cfg.round_cells = int64_t(48) << 20;
+  if (S->cfg.policy != FSLBM_SERVE_ALL && S->cfg.policy != FSLBM_SERVE_LEAST_WORK) {
+    delete S;
+    return fslbm_set_error(FSLBM_ERR_ARG, "server_create: unknown policy %d", cfg->policy);
+  }
   if (int rc = fslbm_ctx_create(device, &S->ctx)) {
     delete S;
     return rc;

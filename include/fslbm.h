@@ -236,15 +236,23 @@ int fslbm_batch_autotune(fslbm_batch* b, int trial_steps, const char* path);
 /* ---- served solves: a request loop with continuous batching (no reference counterpart) ----
  * The server owns a context on `device` and a worker thread. Requests are admitted in arrival
  * order while their device footprint fits the HBM budget (and the resident count its limit);
- * their state stays on the device until they finish. Every round the worker advances all
- * resident solves together, one batched launch per step per storage type, for
- * min(quantum, fewest steps left) steps; requests that arrive meanwhile join at the next
- * round, finished ones leave and free their memory. A solve's result does not depend on what
- * else shares its rounds (the step is bitwise independent of the batch it runs in). */
+ * their state stays on the device until they finish. Every round the worker advances the
+ * round's solves together (batched launches per storage type) for min(quantum, most steps left
+ * among them) steps, each stopping at its own step count; requests that arrive meanwhile join
+ * at the next round, finished ones leave and free their memory. Which resident solves a round
+ * advances is the policy: all of them (FSLBM_SERVE_ALL, the default), or those with the least
+ * work left (box cells x steps left) up to round_cells box cells (FSLBM_SERVE_LEAST_WORK: short
+ * requests overtake long ones, which lowers the median latency for the same total work). A
+ * solve's result does not depend on what else shares its rounds (the step is bitwise
+ * independent of the batch it runs in). */
+enum { FSLBM_SERVE_ALL = 0, FSLBM_SERVE_LEAST_WORK = 1 };
 typedef struct {
   int64_t hbm_budget;  /* bytes of solve state the server may hold; 0 = 150e9 */
   int max_resident;    /* 0 = no limit */
   int quantum;         /* steps per round; 0 = 50 */
+  int policy;          /* FSLBM_SERVE_*; 0 = FSLBM_SERVE_ALL */
+  int64_t round_cells; /* FSLBM_SERVE_LEAST_WORK: box cells per round (at least one request);
+                          0 = 48 Mi */
 } fslbm_server_config;
 
 typedef struct {

@@ -163,3 +163,39 @@ def test_many_admissions_after_retirements(built, ctx):
                 if j % 3 == 0:
                     want, _ = alone(fb, ctx, n, L, re, steps, dt, seed)
                     assert np.array_equal(got, want), (n, L, dt, steps)
+
+
+@pytest.mark.parametrize("policy", ["all", "least_work"])
+def test_round_policy_order(built, ctx, policy):
+    """Request A has more steps but far less work (box cells x steps) than request B. When every
+    round advances every resident request (SERVE_ALL), B, with fewer steps, finishes first; when
+    rounds take the least work first, one request at a time (SERVE_LEAST_WORK, round_cells = 1),
+    A finishes first. Either way both equal the same requests run alone."""
+    fb = built
+    a = (24, 32, 300.0, 120, 1, 41)           # n, L, Re, steps, dtype, seed: 18 Ki cells
+    b = (56, 64, 900.0, 40, 1, 42)            # 196 Ki cells
+    pol = fb.SERVE_ALL if policy == "all" else fb.SERVE_LEAST_WORK
+    with fb.Server(0, quantum=10, policy=pol, round_cells=1) as srv:
+        ids = []
+        for n, L, re, steps, dt, seed in (b, a):
+            dom, R = pipe(fb, n, L)
+            ids.append(srv.submit(dom, params(fb, R, re), dt, steps,
+                                  init_spec=dict(umax=0.2, noise=1e-3, modes=2, mode_amp=0.05,
+                                                 seed=seed)))
+        srv.drain(120)
+        rb, ra = srv.poll(ids[0]), srv.poll(ids[1])
+        assert ra["status"] == rb["status"] == fb.REQ_DONE
+        if policy == "all":
+            assert rb["t_done"] < ra["t_done"]
+        else:
+            assert ra["t_done"] < rb["t_done"]
+        for rid, spec in zip(ids, (b, a)):
+            want, _ = alone(fb, ctx, *spec)
+            assert np.array_equal(srv.release(rid), want)
+
+
+def test_unknown_policy_is_refused(built):
+    fb = built
+    with pytest.raises(fb.FslbmError) as e:
+        fb.Server(0, policy=7)
+    assert e.value.code == -1
