@@ -517,10 +517,10 @@ def _pct(xs, q):
     return float(np.percentile(np.asarray(xs), q)) if xs else None
 
 
-def serve_stream(fb, wl, reqs, policy):
+def serve_stream(fb, wl, reqs, policy, round_cells=0):
     """The seeded request stream submitted in real time to a fresh server with `policy`;
     returns its aggregate MLUPS, latency percentiles and makespan (no fields read back)."""
-    srv = fb.Server(0, hbm_budget=int(150e9), quantum=50, policy=policy)
+    srv = fb.Server(0, hbm_budget=int(150e9), quantum=50, policy=policy, round_cells=round_cells)
     for sp in reqs[:4]:                       # warm-up, not counted
         srv.submit(sp.domain(fb), sp.params(fb), sp.dtype, 20, want_fields=False,
                    init_spec=dict(umax=0.2, seed=1))
