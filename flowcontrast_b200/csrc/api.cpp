@@ -1324,6 +1324,12 @@ static int batch_upload(fslbm_batch* b) {
         const int nout = int((long long)s->L * (c + 1) / nch - (long long)s->L * c / nch);
         for (int t = 0; t < s->ntiles; ++t)
           items.push_back({item_cost(s, t, nout, b->m_w4[i]), make_int2(i, c * s->ntiles + t)});
+        // the chunk's tiles are ordered by the chunk's longest tile, so neighbouring tiles are
+        // claimed one after another and read their shared halo planes while they are in L2
+        int64_t longest = 0;
+        for (size_t k = items.size() - size_t(s->ntiles); k < items.size(); ++k)
+          longest = std::max(longest, items[k].cost);
+        for (size_t k = items.size() - size_t(s->ntiles); k < items.size(); ++k) items[k].cost = longest;
       }
     BatchMon& m = b->h_mons[i];
     std::memset(&m, 0, sizeof m);
