@@ -1705,24 +1705,27 @@ extern "C" int fslbm_batch_autotune(fslbm_batch* b, int trial_steps, const char*
     cur_ms = best.ms;
     table[order[oi].second] = best;
   }
-  // restore
+  // restore every member and free every snapshot even when a step fails; keep the first error
   b->stop = stops;
-  CUDA_TRY(cudaStreamSynchronize(st));
+  cudaError_t re = cudaStreamSynchronize(st);
   for (int i = 0; i < n; ++i) {
     fslbm_solve* s = b->members[i];
     Snap& q = snap[i];
     if (!q.state) continue;
     s->steps = q.steps; s->cur = q.cur; s->launches = q.launches; s->drained = q.drained;
-    CUDA_TRY(cudaMemcpyAsync(s->state[s->cur], q.state, 4 * field_stride(s) * s->es,
-                             cudaMemcpyDeviceToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(s->d_counters, &q.c, sizeof q.c, cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(s->d_gauge, &q.gauge, sizeof q.gauge, cudaMemcpyHostToDevice, st));
-    ctx_free(b->ctx, q.state);
+    if (!re) re = cudaMemcpyAsync(s->state[s->cur], q.state, 4 * field_stride(s) * s->es,
+                                  cudaMemcpyDeviceToDevice, st);
+    if (!re) re = cudaMemcpyAsync(s->d_counters, &q.c, sizeof q.c, cudaMemcpyHostToDevice, st);
+    if (!re) re = cudaMemcpyAsync(s->d_gauge, &q.gauge, sizeof q.gauge, cudaMemcpyHostToDevice, st);
+    ctx_free(b->ctx, q.state);                     // stream-ordered: after the copy
   }
-  CUDA_TRY(cudaMemsetAsync(b->d_tickets + 2, 0, sizeof(unsigned), st));
-  CUDA_TRY(cudaStreamSynchronize(st));             // host snapshots stay alive until copied
+  if (!re) re = cudaMemsetAsync(b->d_tickets + 2, 0, sizeof(unsigned), st);
+  const cudaError_t se = cudaStreamSynchronize(st);  // host snapshots stay alive until copied
+  if (!re) re = se;
   b->h_items.clear();
   if (rc) return rc;
+  if (re) return fslbm_set_error(FSLBM_ERR_CUDA, "batch_autotune: restoring the members: %s",
+                                 cudaGetErrorString(re));
   if (path && !write_tiling(path, table))
     return fslbm_set_error(FSLBM_ERR_IO, "batch_autotune: cannot write %s", path);
   return FSLBM_OK;
