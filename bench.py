@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Benchmark of the plain FSLBM step on one B200 (replicas on N GPUs).
 
-Workload (FP32): periodic pipe of 512 streamwise planes with a 128x128
+Workload (the production pipe, FP32): periodic pipe of 512 streamwise planes with a 128x128
 cross-section, circle R = 63 centred at (63.5, 63.5), paper regime (tblend 0.02, nu 0.0111,
 d1 2, order-4 corrector blend), body force from Re_tau = 180, seeded Poiseuille flow at bulk
 Re ~ 5300 plus random-phase streamwise/azimuthal modes at 10 % of u_bulk. A "step" is one

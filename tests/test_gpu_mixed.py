@@ -88,7 +88,7 @@ def test_fp16_config1_200_steps(built, ctx):
     ref, _ = O.run_core(m2, 64, f, prm, 200, monitor_every=50, radius=15.0)
     got, log = run_gpu(built, ctx, dom, prm, built.F16, f, 200)
     ep, eu, eps = errors(got, ref, m2)
-    print(f"FP16 config-1 pipe, 200 steps: rel L2 u {eu:.3e}, p (scaled) {eps:.3e}")
+    print(f"FP16 small 64x32x32 pipe, 200 steps: rel L2 u {eu:.3e}, p (scaled) {eps:.3e}")
     assert eu <= 3e-3 and eps <= 3e-3, (ep, eu, eps)
     assert [r["step"] for r in log] == [50, 100, 150, 200]
 

@@ -21,7 +21,7 @@ def circle_mask(lx, ly, R, cx, cy):
 
 
 def config1(fb, L=64, lx=32, ly=32, R=15.0, Re=100.0, nu=0.01, noise=1e-3, seed=2024):
-    """64x32x32 (z streamwise), circle R=15 centred at (15.5, 15.5),
+    """The small straight pipe: 64x32x32 (z streamwise), circle R=15 centred at (15.5, 15.5),
     Poiseuille at Re = 2 R u_bulk / nu = 100 plus seeded noise, body force g = 4 nu umax / R^2."""
     cx = cy = (lx - 1) / 2
     umax = 2 * Re * nu / (2 * R)
