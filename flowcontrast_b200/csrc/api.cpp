@@ -715,8 +715,9 @@ extern "C" int fslbm_solve_set_fields(fslbm_solve* s, fslbm_dtype hd, const void
   const size_t n = size_t(s->lx) * s->ly * s->L, hes = hd == FSLBM_F64 ? 8 : 4;
   cudaStream_t st = s->ctx->stream;
   void* dst = s->state[s->cur];
-  if (int(hd) == s->dtype) {
-    // same type: pitched copies straight into the state
+  if (int(hd) == s->dtype && s->lx == s->lxp) {
+    // same type and no pitch padding: one contiguous copy per field straight into the state
+    // (narrow pitched rows would make slow DMA; those go through the staging buffer)
     const void* src[4] = {p, u, v, w};
     for (int f = 0; f < 4; ++f)
       CUDA_TRY(cudaMemcpy2DAsync(static_cast<char*>(dst) + f * field_stride(s) * s->es,
@@ -771,8 +772,9 @@ extern "C" int fslbm_solve_init_poiseuille(fslbm_solve* s, double umax, double n
 }
 
 // Device bytes fslbm_solve_create allocates for this domain and dtype (state ping-pong, mask,
-// column sums, tile list, monitor log and small buffers); a host-type read-back of a solve
-// whose storage type differs adds a staging buffer of 4 fields in that type.
+// column sums, tile list, monitor log and small buffers). Host-layout copies in or out
+// (set/get fields) of a solve whose storage type differs from the host type, or whose width is
+// not a multiple of 8, add a staging buffer of 4 fields in the host type.
 extern "C" int fslbm_solve_footprint(const fslbm_domain* dom, fslbm_dtype dtype, int64_t* bytes) {
   if (!dom || !bytes || dom->lx < 1 || dom->ly < 1 || dom->lz < 1)
     return fslbm_set_error(FSLBM_ERR_ARG, "solve_footprint: bad argument");
@@ -799,7 +801,7 @@ extern "C" int fslbm_solve_get_fields(fslbm_solve* s, fslbm_dtype hd, void* p, v
   cudaStream_t st = s->ctx->stream;
   const void* src = s->state[s->cur];
   void* dst[4] = {p, u, v, w};
-  if (int(hd) == s->dtype) {
+  if (int(hd) == s->dtype && s->lx == s->lxp) {
     for (int f = 0; f < 4; ++f)
       CUDA_TRY(cudaMemcpy2DAsync(dst[f], size_t(s->lx) * hes,
                                  static_cast<const char*>(src) + f * field_stride(s) * s->es,

@@ -550,22 +550,32 @@ cudaError_t launch_zero_walls(int dtype, void* state, const uint8_t* mask, int p
   return cudaGetLastError();
 }
 
+// Dense host-layout fields (4 x L x ly x lx) <-> the pitched state (4 x L x ly x lxp), with a type
+// conversion. A warp copies one row at a time (one division per row, coalesced along x).
 template <class TS, class TH>
 __global__ void convert_in_kernel(TS* s, const TH* src, int lx, int lxp, int ly, int L) {
-  const size_t n = size_t(lx) * ly * L, FS = size_t(lxp) * ly * L;
-  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < 4 * n;
-       i += size_t(gridDim.x) * blockDim.x) {
-    const size_t f = i / n, r = i % n, x = r % lx, yz = r / lx;
-    s[f * FS + yz * lxp + x] = TS(src[i]);
+  const long long rows = (long long)ly * L, FS = (long long)lxp * rows;
+  const int lane = threadIdx.x & 31;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long rr = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; rr < 4 * rows;
+       rr += nwarps) {
+    const long long f = rr / rows, yz = rr - f * rows;
+    const TH* in = src + rr * lx;
+    TS* out = s + f * FS + yz * lxp;
+    for (int x = lane; x < lx; x += 32) out[x] = TS(in[x]);
   }
 }
 template <class TS, class TH>
 __global__ void convert_out_kernel(const TS* s, TH* dst, int lx, int lxp, int ly, int L) {
-  const size_t n = size_t(lx) * ly * L, FS = size_t(lxp) * ly * L;
-  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < 4 * n;
-       i += size_t(gridDim.x) * blockDim.x) {
-    const size_t f = i / n, r = i % n, x = r % lx, yz = r / lx;
-    dst[i] = TH(s[f * FS + yz * lxp + x]);
+  const long long rows = (long long)ly * L, FS = (long long)lxp * rows;
+  const int lane = threadIdx.x & 31;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long rr = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; rr < 4 * rows;
+       rr += nwarps) {
+    const long long f = rr / rows, yz = rr - f * rows;
+    const TS* in = s + f * FS + yz * lxp;
+    TH* out = dst + rr * lx;
+    for (int x = lane; x < lx; x += 32) out[x] = TH(in[x]);
   }
 }
 

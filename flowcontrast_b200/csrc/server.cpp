@@ -378,7 +378,9 @@ extern "C" int fslbm_server_submit(fslbm_server* S, const fslbm_request* req, in
   r->has_out = all_out;
   int64_t bytes = 0;
   if (int rc = fslbm_solve_footprint(&d, fslbm_dtype(req->dtype), &bytes)) return rc;
-  if (all_out && req->dtype != FSLBM_F32) bytes += 16 * r->res.cells;   // read-back staging
+  // host start in or fields out go through a staging buffer (4 FP32 fields) unless the state is
+  // FP32 without pitch padding
+  if ((all_out || all_init) && (req->dtype != FSLBM_F32 || d.lx % 8 != 0)) bytes += 16 * r->res.cells;
   r->res.bytes_device = bytes;
   if (bytes > S->cfg.hbm_budget)
     return fslbm_set_error(FSLBM_ERR_BUDGET, "server_submit: footprint %lld B exceeds the budget %lld B",

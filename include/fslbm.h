@@ -170,7 +170,9 @@ int fslbm_solve_init_poiseuille(fslbm_solve* s, double umax, double noise, int m
 /* Corrector coefficients c0..c8 of an order and blend as the solve of `dtype` uses them (FP32
  * forms for FP32 and FP16 storage); *taps = K. FSLBM_ERR_ARG for an unknown order. */
 int fslbm_fd_coefficients(int order, double blend, fslbm_dtype dtype, double* c, int* taps);
-/* Device bytes fslbm_solve_create allocates for a domain and dtype (an upper bound). */
+/* Device bytes fslbm_solve_create allocates for a domain and dtype (an upper bound). Copying
+ * host-layout fields in or out later adds a staging buffer of 4 fields in the host type when the
+ * storage type differs from the host type or lx is not a multiple of 8. */
 int fslbm_solve_footprint(const fslbm_domain* dom, fslbm_dtype dtype, int64_t* bytes);
 
 /* ---- reference-layout fields: the core plus d2 buffer planes at each streamwise end,
