@@ -132,6 +132,12 @@ def test_server_without_gpu_reports_error(built):
     assert e.value.code == -2
 
 
+def test_server_refuses_unknown_policy_before_touching_a_device(built):
+    with pytest.raises(built.FslbmError) as e:
+        built.Server(0, policy=7)
+    assert e.value.code == -1
+
+
 def test_solve_footprint_counts_state_ping_pong(built):
     import ctypes
     fb = built

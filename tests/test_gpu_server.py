@@ -193,9 +193,3 @@ def test_round_policy_order(built, ctx, policy):
             want, _ = alone(fb, ctx, *spec)
             assert np.array_equal(srv.release(rid), want)
 
-
-def test_unknown_policy_is_refused(built):
-    fb = built
-    with pytest.raises(fb.FslbmError) as e:
-        fb.Server(0, policy=7)
-    assert e.value.code == -1
