@@ -165,3 +165,32 @@ def test_reconfigured_member_is_refused(built, ctx):
     b.close()
     for s in members:
         s.close()
+
+
+@pytest.mark.parametrize("chain", ["1", "5"])
+def test_chain_length_does_not_change_results(built, ctx, monkeypatch, chain):
+    """Steps per chained launch (FSLBM_BATCH_CHAIN; odd values run as the next even count) only
+    decide where launches end: 2 or 6 steps per launch, graph replays plus a remainder launch,
+    give each member's own plain-path result bit for bit, monitors included."""
+    fb = built
+    monkeypatch.setenv("FSLBM_BATCH_CHAIN", chain)
+    specs = member_specs(n=4, seed=57)
+    steps = 53
+    alone = []
+    for sp in specs:
+        s = make_member(fb, ctx, sp)
+        s.step(steps)
+        s.sync()
+        alone.append((s.get_fields(np.float32), [r["q1"] for r in s.monitor_log()]))
+        s.close()
+    members = [make_member(fb, ctx, sp) for sp in specs]
+    b = fb.Batch(ctx, members)
+    b.step(steps)
+    b.sync()
+    for s, (want, q1) in zip(members, alone):
+        assert np.array_equal(s.get_fields(np.float32), want)
+        assert [r["q1"] for r in s.monitor_log()] == q1
+        assert s.info()["steps"] == steps
+    b.close()
+    for s in members:
+        s.close()
