@@ -36,7 +36,8 @@ static cudaError_t launch_step_t(const StepLaunch& a, cudaStream_t st) {
   for (int j = 0; j < 6; ++j) k.ch[j] = TC(a.ch[j]);
   k.fx = TC(a.fx); k.fy = TC(a.fy); k.fz = TC(a.fz);
   const int grid = a.ntiles * a.nchunks;
-  fslbm_step_kernel<TS, D1, K><<<grid, kThreads, Tl::SMEM_BYTES, st>>>(*a.map, g, k);
+  if (a.mask_planes > 1) fslbm_step_kernel<TS, D1, K, true><<<grid, kThreads, Tl::SMEM_BYTES, st>>>(*a.map, g, k);
+  else fslbm_step_kernel<TS, D1, K, false><<<grid, kThreads, Tl::SMEM_BYTES, st>>>(*a.map, g, k);
   return cudaGetLastError();
 }
 
@@ -66,10 +67,15 @@ size_t step_smem_bytes(int dtype, int d1, int K) {
 
 cudaError_t step_prepare(int dtype, int d1, int K) {
 #define X(DT, TS, D, KK)                                                                        \
-  if (dtype == DT && d1 == D && K == KK)                                                        \
-    return cudaFuncSetAttribute(fslbm_step_kernel<TS, D, KK>,                                   \
+  if (dtype == DT && d1 == D && K == KK) {                                                      \
+    cudaError_t e = cudaFuncSetAttribute(fslbm_step_kernel<TS, D, KK, false>,                   \
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,           \
+                                         int(StepTile<TS, D, KK>::SMEM_BYTES));                 \
+    if (e) return e;                                                                            \
+    return cudaFuncSetAttribute(fslbm_step_kernel<TS, D, KK, true>,                             \
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,                    \
-                                int(StepTile<TS, D, KK>::SMEM_BYTES));
+                                int(StepTile<TS, D, KK>::SMEM_BYTES));                          \
+  }
   FSLBM_STEP_COMBOS(X)
 #undef X
   return cudaErrorInvalidValue;

@@ -73,13 +73,16 @@ struct StepGeom {
   const uint8_t* mask;     // lxp*ly per plane: 0 fluid, 125 wall (padding columns are wall)
   const void* colcoef;     // ColCoef<TC>[lxp*ly], or CellCoef<TC>[lxp*ly*L] for mask_planes > 1
   int mask_planes;         // 0 or 1: one cross-section extruded along z; L: one per plane
+                           // (the kernel's MP parameter must match: MP = mask_planes > 1)
   void* out;               // output state: 4 fields, field stride lxp*ly*L
   const double* gauge;     // p2 of the previous monitor (applied this step) or null
   unsigned* err;           // bit 0: a bounded wait gave up
   long long* step_counter; // device step count, advanced by block 0
 };
 
-template <class TS, int D1, int K = 2>
+// MP: masks that vary along z (one cross-section and per-cell wall sums per plane). A template
+// parameter rather than a runtime test: the test sat in per-element loops and cost 17 % in FP64.
+template <class TS, int D1, int K = 2, bool MP = false>
 __global__ void __launch_bounds__(kThreads, sizeof(TS) == 8 ? 1 : 2)
     fslbm_step_kernel(const __grid_constant__ CUtensorMap tin, const StepGeom g,
                       const StepConst<typename Compute<TS>::type> k) {
@@ -114,7 +117,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(TS) == 8 ? 1 : 2)
   }
   bool fluid = false;
   TC ws0 = 0, wsx = 0, wsy = 0;
-  if (x < g.lxp && y < g.ly && g.mask_planes <= 1) {
+  if (x < g.lxp && y < g.ly && !MP) {
     const ColCoef<TC> c = reinterpret_cast<const ColCoef<TC>*>(g.colcoef)[y * g.lxp + x];
     fluid = c.fluid != TC(0);
     ws0 = c.ws0; wsx = c.wsx; wsy = c.wsy;
@@ -162,7 +165,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(TS) == 8 ? 1 : 2)
       const TC off = sp < 0 ? k.pin : (sp >= g.L ? -k.pin : TC(0));
       // a mask per plane: the seam offset goes on the non-wall cells of the wrapped plane
       const uint8_t* mz = nullptr;
-      if (g.mask_planes > 1 && off != TC(0)) {
+      if (MP && off != TC(0)) {
         int zz = sp % g.L;
         if (zz < 0) zz += g.L;
         mz = g.mask + size_t(zz) * g.lxp * g.ly;
@@ -249,7 +252,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(TS) == 8 ? 1 : 2)
 
     const int zo = t - R;   // output plane; its predictor sums completed just above
     TC wsz = 0;
-    if (g.mask_planes > 1 && zo >= zb && x < g.lxp && y < g.ly) {
+    if (MP && zo >= zb && x < g.lxp && y < g.ly) {
       const size_t cell = (size_t(zo) * g.ly + y) * g.lxp + x;
       fluid = g.mask[cell] == 0;
       const CellCoef<TC> c = reinterpret_cast<const CellCoef<TC>*>(g.colcoef)[cell];
