@@ -40,6 +40,12 @@ def physics():
     return ub, 2 * ub, 2 * ut * ut / W["R"]
 
 
+def fluid_fraction():
+    """Share of the box cells that are fluid (the circle of radius R in the cross-section)."""
+    y, x = np.mgrid[0:W["ly"], 0:W["lx"]]
+    return float(np.count_nonzero((x - W["cx"]) ** 2 + (y - W["cy"]) ** 2 <= W["R"] ** 2)) / (W["lx"] * W["ly"])
+
+
 def workload_config(extra=None):
     ub, umax, g = physics()
     c = {"workload": "plain FSLBM FP32, periodic pipe 512 (z, streamwise) x 128 x 128, R=63, "
@@ -136,20 +142,6 @@ class ClockSampler:
                 "samples": len(inside)}
 
 
-def read_traffic(summary="fslbm_step2_f32_512x128x128.md", key="dram_bytes_per_launch_full_size"):
-    """DRAM bytes (read + write) from a committed ncu summary under profiles/, if present."""
-    path = os.path.join(ROOT, "profiles", summary)
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        if line.strip().startswith(key + ":"):
-            try:
-                return float(line.split(":", 1)[1].split()[0])
-            except ValueError:
-                return None
-    return None
-
-
 def hbm_peak():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -158,15 +150,29 @@ def hbm_peak():
         return 6650.0, "fallback"
 
 
+def _oracle():
+    """The test-only oracle library (the CPU restatement of the reference step); the CPU legs
+    of the benchmark use it and never load the solver library."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    return O
+
+
+def seeded_start(O, planes, seed_offset=0):
+    """The workload's seeded start on `planes` streamwise planes, (4, planes, ly, lx) float64,
+    from the oracle's generator (bitwise equal to the library's fslbm_init_poiseuille)."""
+    ub, umax, g = physics()
+    return O.init_poiseuille(W["lx"], W["ly"], planes, W["R"], W["cx"], W["cy"], umax,
+                             noise=1e-3, modes=4, mode_amp=0.1 * ub / umax,
+                             seed=W["seed"] + seed_offset)
+
+
 def cpu_port_sample(seconds=10.0, planes=64, nthreads=0):
     """The oracle's FP32 restatement of the reference step on the host cores, on a bounded
     streamwise slice of the workload (same cross-section and parameters)."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_lib as O
-    import flowcontrast_b200 as fb
+    O = _oracle()
     ub, umax, g = physics()
-    dom = fb.make_domain(W["lx"], W["ly"], planes, radius=W["R"], cx=W["cx"], cy=W["cy"])
-    f = fb.init_poiseuille(dom, umax, noise=1e-3, modes=4, mode_amp=0.1 * ub / umax, seed=W["seed"])
+    f = seeded_start(O, planes)
     y, x = np.mgrid[0:W["ly"], 0:W["lx"]]
     m2 = np.where((x - W["cx"]) ** 2 + (y - W["cy"]) ** 2 <= W["R"] ** 2, 0, 125).astype(np.uint8)
     prm = dict(tblend=W["tblend"], pin=0.0, nu=W["nu"], d1=W["d1"], blend=W["blend"],
@@ -203,18 +209,14 @@ def reference_gpu_sample(steps=20):
             return None
     except ImportError:
         return None
-    import flowcontrast_b200 as fb
     lib = ctypes.CDLL(path)
     u8 = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
     f32 = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
     i = ctypes.c_int
     lib.ref_run.argtypes = [u8, i, i, i, i, f32, f32, f32, i, ctypes.POINTER(ctypes.c_float),
                             ctypes.POINTER(ctypes.c_uint)]
-    ub, umax, g = physics()
     d2, L = 10, W["lz"]
-    dom = fb.make_domain(W["lx"], W["ly"], L, radius=W["R"], cx=W["cx"], cy=W["cy"])
-    core = fb.init_poiseuille(dom, umax, noise=1e-3, modes=4, mode_amp=0.1 * ub / umax,
-                              seed=W["seed"]).astype(np.float32)
+    core = seeded_start(_oracle(), L).astype(np.float32)
     f = np.concatenate([core[:, -d2:], core, core[:, :d2]], axis=1)
     y, x = np.mgrid[0:W["ly"], 0:W["lx"]]
     fluid = (x - W["cx"]) ** 2 + (y - W["cy"]) ** 2 <= W["R"] ** 2
@@ -239,18 +241,14 @@ def run_reference_arm(args, rank, world, local):
     host cores, rank 0 only, on a bounded slice per step."""
     if rank != 0:
         return 0
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_lib as O
-    import flowcontrast_b200 as fb
+    O = _oracle()
     ub, umax, g = physics()
     threads = O.threads()
     # size the per-step slice so the whole run stays within about two minutes
     _, t_step64 = cpu_port_sample(seconds=0.0, planes=64, nthreads=threads)
     budget = 100.0 / max(1, args.steps + args.warmup)
     planes = int(max(6, min(W["lz"], 64 * budget / max(t_step64, 1e-6))))
-    dom = fb.make_domain(W["lx"], W["ly"], planes, radius=W["R"], cx=W["cx"], cy=W["cy"])
-    f = fb.init_poiseuille(dom, umax, noise=1e-3, modes=4, mode_amp=0.1 * ub / umax,
-                           seed=W["seed"]).astype(np.float32)
+    f = seeded_start(O, planes).astype(np.float32)
     y, x = np.mgrid[0:W["ly"], 0:W["lx"]]
     m2 = np.where((x - W["cx"]) ** 2 + (y - W["cy"]) ** 2 <= W["R"] ** 2, 0, 125).astype(np.uint8)
     prm = dict(tblend=W["tblend"], pin=0.0, nu=W["nu"], d1=W["d1"], blend=W["blend"],
@@ -269,10 +267,11 @@ def run_reference_arm(args, rank, world, local):
               f"of the workload on {threads} host threads (oracle restatement of FSLBM.cu; the "
               "reference has no CPU implementation and its CUDA source predates CUDA 12)")
     line = {"metric": METRIC, "value": mlups, "unit": "MLUPS", "impl": "reference",
+            "fluid_mlups": mlups * fluid_fraction(),
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config({"sample_planes": planes}),
+            "config": workload_config(), "sample_planes": planes,
             "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0,
@@ -352,6 +351,7 @@ def run_ours(args, rank, world, local):
       e2e = {"value": world * cells * E2E_INNER * reps / e2e_s / 1e6, "unit": "MLUPS",
              "h2d_bytes_per_step": state_bytes / E2E_INNER,
              "d2h_bytes_per_step": (state_bytes + (E2E_INNER // 50) * 64) / E2E_INNER,
+             "request_steps": E2E_INNER,
              "request": f"H2D of the FP32 state from pinned memory + {E2E_INNER} steps + "
                         "monitor read-back + D2H of the state, via fslbm_solve_set_fields/step/"
                         "monitor/get_fields"}
@@ -361,17 +361,20 @@ def run_ours(args, rank, world, local):
         kern_avg_ms = kern_ms / max(kern_n, 1)
         alg_bytes = 32.0 * cells                  # read p,u,v,w + write p,u,v,w, FP32
         achieved = alg_bytes / (kern_avg_ms * 1e-3) / 1e9
-        traffic = read_traffic()
         cpu, _ = cpu_port_sample(seconds=args.cpu_seconds) if args.cpu_seconds > 0 else (None, 0)
         value = world * cells * args.steps / (ms * 1e-3) / 1e6
         line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world,
+                "fluid_mlups": value * fluid_fraction(),
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": value / PUBLISHED_MLUPS, "dtype": "f32",
                 "data": "synthetic (seeded Poiseuille + random-phase modes)",
-                "config": workload_config({"e2e_request_steps": E2E_INNER}),
+                "config": workload_config(),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": traffic,
+                             "frac": achieved / peak, "traffic": None,
+                             "traffic_note": "DRAM counters need a profiler, so the run does not "
+                                             "measure them; per-launch DRAM bytes of ncu captures "
+                                             "are in profiles/",
                              "peak_source": f"{peak_kind} hbm_gbs",
                              "kernel": "fslbm_step2_kernel<2,32,packed>",
                              "kernel_ms_avg": kern_avg_ms, "algorithmic_bytes": alg_bytes},
@@ -496,9 +499,7 @@ def run_ensemble(args):
             "batch_equals_plain_bitwise": bool(same),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": read_traffic("fslbm_step2_batch_kernel_ensemble64.md",
-                                                 "dram_bytes_per_step_full_size"),
-                         "traffic_unit": "bytes per ensemble step (one step of the chained launch)",
+                         "traffic": None,
                          "peak_source": f"{peak_kind} hbm_gbs",
                          "kernel": "fslbm_step2_batch_kernel<2,32,scalar,float> (chained steps)"},
             "e2e": {"value": cells * args.steps / e2e_s / 1e6, "unit": "MLUPS",

@@ -504,3 +504,64 @@ int oracle_max_threads(void) {
 }
 
 }  // extern "C"
+
+// ---- seeded starting fields of the benchmark workloads ----
+// The benchmark's CPU arms (the timed CPU baseline and the reference arm) start from the same
+// seeded state as the GPU arm but must not load the solver library, so the generator is
+// restated here: a circular pipe of radius R centred at (cx, cy) (fluid iff
+// (x-cx)^2 + (y-cy)^2 <= R^2), p = 0, stored w = -umax (1 - s^2) with s = r/R, uniform noise
+// of amplitude noise*umax on u, v, w, and `modes` random-phase streamwise/azimuthal sinusoids
+// of amplitude mode_amp*umax under the envelope 2.6 s (1 - s^2). Random numbers are
+// splitmix64 (Steele, Lea and Flood, 2014) of the seed, xor-ed with a counter (4*cell + k,
+// cell = x + lx*(y + ly*z)), mapped to [-1, 1) from the top 53 bits. The expressions are
+// evaluated in the same order as the library's generator, so the two agree bit for bit (a CPU
+// test checks this).
+namespace {
+uint64_t oracle_splitmix(uint64_t x) {
+  uint64_t z = x + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+double oracle_unit(uint64_t seed, uint64_t counter) {
+  return double(oracle_splitmix(oracle_splitmix(seed) ^ counter) >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+}  // namespace
+
+extern "C" int oracle_init_poiseuille(int lx, int ly, int L, double R, double cx, double cy,
+                                      double umax, double noise, int modes, double mode_amp,
+                                      uint64_t seed, double* out) {
+  if (lx < 1 || ly < 1 || L < 1 || R <= 0 || modes < 0 || modes > 16 || !out) return -1;
+  const double pi = 3.14159265358979323846;
+  double ph[64];
+  for (int m = 0; m < modes; ++m)
+    for (int k = 0; k < 4; ++k) ph[4 * m + k] = pi * (1.0 + oracle_unit(seed ^ 0xA5A5A5A5ull, 4ull * m + k));
+  const long nc = long(lx) * ly * L;
+  const double a = noise * umax, b = mode_amp * umax;
+  for (int z = 0; z < L; ++z)
+    for (int y = 0; y < ly; ++y)
+      for (int x = 0; x < lx; ++x) {
+        const long i = x + long(lx) * (y + long(ly) * z);
+        const double dx = x - cx, dy = y - cy;
+        double f[4] = {0.0, 0.0, 0.0, 0.0};
+        if (dx * dx + dy * dy <= R * R) {
+          const uint64_t idx = uint64_t(i);
+          const double s2 = (dx * dx + dy * dy) / (R * R), s = std::sqrt(s2);
+          const double th = std::atan2(dy, dx);
+          double du = a * oracle_unit(seed, 4 * idx + 1);
+          double dv = a * oracle_unit(seed, 4 * idx + 2);
+          double dw = a * oracle_unit(seed, 4 * idx + 3);
+          const double env = 2.6 * s * (1.0 - std::fmin(s2, 1.0));
+          for (int m = 0; m < modes; ++m) {
+            const double kz = 2.0 * pi * double(m + 1) * z / double(L);
+            const int n = 1 + m % 4;
+            dw += b * env * std::sin(kz + ph[4 * m]) * std::cos(n * th + ph[4 * m + 1]);
+            du += b * env * std::cos(kz + ph[4 * m + 2]) * std::sin(n * th + ph[4 * m + 3]);
+            dv += b * env * std::sin(kz + ph[4 * m + 2]) * std::cos(n * th + ph[4 * m + 3]);
+          }
+          f[1] = du; f[2] = dv; f[3] = -umax * std::fmax(0.0, 1.0 - s2) + dw;
+        }
+        for (int k = 0; k < 4; ++k) out[k * nc + i] = f[k];
+      }
+  return 0;
+}

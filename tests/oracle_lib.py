@@ -44,6 +44,7 @@ def lib():
         L.oracle_pipe_m_mask.argtypes = [i, i, i, _u8p]
         L.oracle_max_threads.argtypes = []
         L.oracle_fd_coefficients.argtypes = [i, d, _f64p]
+        L.oracle_init_poiseuille.argtypes = [i, i, i, d, d, d, d, d, i, d, ctypes.c_uint64, _f64p]
         _lib = L
     return _lib
 
@@ -113,6 +114,17 @@ def stats_accumulate(acc, p, u, v, w, cnt):
     n = p.size
     lib().oracle_stats_accumulate(n, *(np.ascontiguousarray(a, np.float64).ravel() for a in (p, u, v, w)),
                                   int(cnt), acc.ravel())
+
+
+def init_poiseuille(lx, ly, L, radius, cx, cy, umax, noise=0.0, modes=0, mode_amp=0.0, seed=0):
+    """Seeded start of the benchmark workloads on a circular pipe, (4, L, ly, lx) float64; the
+    same fields as the library's fslbm_init_poiseuille, without loading the library."""
+    out = np.zeros(4 * L * ly * lx)
+    rc = lib().oracle_init_poiseuille(lx, ly, L, float(radius), float(cx), float(cy), float(umax),
+                                      float(noise), int(modes), float(mode_amp), int(seed), out)
+    if rc:
+        raise ValueError(f"oracle_init_poiseuille rejected the case: code {rc}")
+    return out.reshape(4, L, ly, lx)
 
 
 def fd_coefficients(order, blend=0.0):
