@@ -44,10 +44,15 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 EncodeTiledFn g_encode = nullptr;
 
+// Error word bits: the step kernel's bounded waits set bit 0; the mask check sets bit 1.
+constexpr unsigned kErrBadMask = 2u;
+
 // Per-column wall sums (the same arithmetic, in the same order, as the solve's host-side
-// table), the tile list (every tile of the padded cross-section), the gauge and a cleared
-// error flag, written into the scratch array.
-__global__ void noalloc_prepare(const uint8_t* mask, int lxp, int ly, int ntx, int ntiles,
+// table), the tile list (every tile of the padded cross-section) and the gauge, written into
+// the scratch array (the host clears the error word first). The mask must hold only 0 and 125,
+// with wall on the cross-section rim and in the padding columns (the conditions the solve
+// checks at creation); anything else sets kErrBadMask.
+__global__ void noalloc_prepare(const uint8_t* mask, int lx, int lxp, int ly, int ntx, int ntiles,
                                 double gauge, unsigned char* scratch) {
   ColCoef<float>* cc = reinterpret_cast<ColCoef<float>*>(scratch);
   int2* tiles = reinterpret_cast<int2*>(scratch + kCoefBytes);
@@ -68,13 +73,20 @@ __global__ void noalloc_prepare(const uint8_t* mask, int lxp, int ly, int ntx, i
     c.ws0 = float(a); c.wsx = float(bx); c.wsy = float(by);
     c.fluid = mask[i] == 0 ? 1.0f : 0.0f;
     cc[i] = c;
+    const uint8_t m = mask[i];
+    const bool rim = x == 0 || y == 0 || x >= lx - 1 || y == ly - 1;
+    if ((m != 0 && m != kWall) || (m == 0 && rim))
+      atomicOr(reinterpret_cast<unsigned*>(scratch + kErrOffset), kErrBadMask);
   }
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x)
     tiles[t] = make_int2(kTX * (t % ntx), kNoallocTY * (t / ntx));
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    *reinterpret_cast<double*>(scratch + kGaugeOffset) = gauge;
-    *reinterpret_cast<unsigned*>(scratch + kErrOffset) = 0u;
-  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *reinterpret_cast<double*>(scratch + kGaugeOffset) = gauge;
+}
+
+// [a, a + na) and [b, b + nb) share a byte
+bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
+  const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+  return x < y + nb && y < x + na;
 }
 
 // Once per device, with that device current: the scratch array's device address, the
@@ -131,6 +143,12 @@ extern "C" int fslbm_step_f32_noalloc(const float* state_in, float* state_out,
   const int ntx = (lx_pitch + kTX - 1) / kTX, nty = (ly + kNoallocTY - 1) / kNoallocTY;
   if (ntx * nty > kNoallocMaxTiles)
     return fslbm_set_error(FSLBM_ERR_ARG, "step_f32_noalloc: too many tiles");
+  // the step reads state_in by TMA while other CTAs write state_out: they must not overlap
+  const size_t state_bytes = 4 * size_t(lx_pitch) * ly * lz * sizeof(float);
+  if (overlaps(state_in, state_bytes, state_out, state_bytes) ||
+      overlaps(mask, size_t(lx_pitch) * ly, state_out, state_bytes))
+    return fslbm_set_error(FSLBM_ERR_ARG,
+                           "step_f32_noalloc: state_out overlaps state_in or mask (the step is not in place)");
 
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -140,7 +158,9 @@ extern "C" int fslbm_step_f32_noalloc(const float* state_in, float* state_out,
   unsigned char* scratch = static_cast<unsigned char*>(g_scratch_ptr[dev]);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
 
-  noalloc_prepare<<<64, 256, 0, st>>>(mask, lx_pitch, ly, ntx, ntx * nty, gauge, scratch);
+  if ((e = cudaMemsetAsync(scratch + kErrOffset, 0, sizeof(unsigned), st)) != cudaSuccess)
+    return fslbm_set_error(FSLBM_ERR_CUDA, "step_f32_noalloc: %s", cudaGetErrorString(e));
+  noalloc_prepare<<<64, 256, 0, st>>>(mask, lx, lx_pitch, ly, ntx, ntx * nty, gauge, scratch);
   if ((e = cudaGetLastError()) != cudaSuccess)
     return fslbm_set_error(FSLBM_ERR_CUDA, "step_f32_noalloc: prepare: %s", cudaGetErrorString(e));
 
@@ -201,6 +221,10 @@ extern "C" int fslbm_step_f32_noalloc(const float* state_in, float* state_out,
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess)
     return fslbm_set_error(FSLBM_ERR_CUDA, "step_f32_noalloc: %s", cudaGetErrorString(e));
+  if (err & kErrBadMask)
+    return fslbm_set_error(FSLBM_ERR_ARG,
+                           "step_f32_noalloc: mask values must be 0 or 125, with wall on the rim and "
+                           "in the padding columns (state_out is not a valid step)");
   if (err)
     return fslbm_set_error(FSLBM_ERR_TIMEOUT, "step_f32_noalloc: a bounded device wait gave up");
   return FSLBM_OK;

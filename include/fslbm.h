@@ -321,9 +321,12 @@ int fslbm_server_stats_get(fslbm_server* srv, fslbm_server_stats* out);
  * fail under memory pressure) is not allowed.
  *  - state_in, state_out: device arrays of 4 fields (p,u,v,w), each lz*ly*lx_pitch floats, x
  *    fastest, field stride lz*ly*lx_pitch; 16-byte aligned; lx_pitch a multiple of 8, >= lx.
- *    Wall cells and the padding columns x >= lx must hold zero in state_in; the step does not
- *    write them in state_out, so keep them zero there too (for example by zeroing it once).
- *  - mask: device array of ly*lx_pitch bytes, 0 fluid / 125 wall; padding columns are wall.
+ *    They must not overlap (the step is not in place: FSLBM_ERR_ARG). Wall cells and the
+ *    padding columns x >= lx must hold zero in state_in; state_out gets zero there.
+ *  - mask: device array of ly*lx_pitch bytes, 0 fluid / 125 wall, with wall on the rim of the
+ *    lx x ly cross-section and in the padding columns. The mask is checked on the device during
+ *    the call; a mask that breaks these rules gives FSLBM_ERR_ARG, and state_out then holds no
+ *    valid step.
  *  - gauge: p2 subtracted from p this step (0 outside the step after a monitor).
  *  - stream: the caller's cudaStream_t (NULL for the default stream). The call returns after
  *    the step has finished on that stream.

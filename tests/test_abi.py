@@ -150,3 +150,37 @@ def test_solve_footprint_counts_state_ping_pong(built):
     state = 2 * 4 * 128 * 128 * 512
     for dt, es in ((fb.F64, 8), (fb.F32, 4), (fb.F16, 2)):
         assert state * es <= out[dt] <= state * es + 4 * 2 ** 20
+
+
+def test_noalloc_argument_checks_need_no_device(built):
+    """fslbm_step_f32_noalloc refuses, before touching a device: a cross-section beyond its
+    65 536-cell scratch, d1 != 2, and an output that overlaps the input or the mask (the step
+    reads its input while other blocks write the output, so it cannot run in place). The
+    pointers are never dereferenced on these paths."""
+    import ctypes
+    fb = built
+    fn = fb.lib().fslbm_step_f32_noalloc
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                   ctypes.c_int, ctypes.c_int, ctypes.POINTER(fb.Params), ctypes.c_double,
+                   ctypes.c_void_p]
+    prm = fb.Params.make(d1=2, blend=1.0)
+    lx, ly, lz, pitch = 32, 32, 40, 32
+    nbytes = 4 * lz * ly * pitch * 4
+    a, b, m = 1 << 32, (1 << 32) + 2 * nbytes, (1 << 32) + 4 * nbytes
+    buf = ctypes.create_string_buffer(256)
+
+    def call(*args, **kw):
+        rc = fn(*args, ctypes.byref(kw.get("prm", prm)), 0.0, None)
+        fb.lib().fslbm_last_error(buf, 256)
+        return rc, buf.value.decode()
+
+    rc, msg = call(a, b, m, 264, 256, lz, 264)           # 264 * 256 > 65536 cells
+    assert rc == -1 and "65536" in msg
+    rc, msg = call(a, b, m, lx, ly, lz, pitch, prm=fb.Params.make(d1=3))
+    assert rc == -1 and "d1" in msg
+    rc, msg = call(a, a, m, lx, ly, lz, pitch)           # in place
+    assert rc == -1 and "overlaps" in msg
+    rc, msg = call(a, a + nbytes // 2, m, lx, ly, lz, pitch)   # partly overlapping
+    assert rc == -1 and "overlaps" in msg
+    rc, msg = call(a, b, b + 64, lx, ly, lz, pitch)      # mask inside the output
+    assert rc == -1 and "overlaps" in msg
