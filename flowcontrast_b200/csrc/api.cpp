@@ -214,9 +214,9 @@ struct fslbm_solve {
   double* d_gauge = nullptr;
   unsigned* d_err = nullptr;
   double* d_scratch = nullptr;     // small reductions
-  double* d_stats = nullptr;       // 11 * ly * (L + 2 d2)
+  double* d_stats = nullptr;       // 11 * ly * (L + 2 d2) sums, then their 11 compensations
   int cnt = 0, cnt2 = 0;
-  double* d_prof = nullptr;        // 10 * lxp * ly
+  double* d_prof = nullptr;        // 10 * lxp * ly sums, then their 10 compensations
   int64_t prof_n = 0;
   void* d_stage = nullptr;         // conversion staging (dense 4 fields)
   size_t stage_bytes = 0;
@@ -908,6 +908,7 @@ extern "C" int fslbm_solve_step(fslbm_solve* s, int64_t nsteps) {
   if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "step: null solve");
   if (nsteps < 0) return fslbm_set_error(FSLBM_ERR_ARG, "step: negative step count");
   if (!s->fields_set) return fslbm_set_error(FSLBM_ERR_STATE, "step: fields were never set");
+  NvtxRange range("fslbm_solve_step");
   CUDA_TRY(cudaSetDevice(s->ctx->device));
   CUDA_TRY(cudaEventRecord(s->ev0, s->ctx->stream));
   if (int r = enqueue_steps(s, nsteps)) return r;
@@ -1109,13 +1110,14 @@ extern "C" int fslbm_solve_get_plane(fslbm_solve* s, int kind, int comp, float* 
 static int ensure_stats(fslbm_solve* s) {
   if (s->d_stats) return FSLBM_OK;
   const size_t n = size_t(s->ly) * (s->L + 2 * s->d2);
-  CUDA_TRY(dalloc(s, &s->d_stats, 11 * n * sizeof(double)));
-  CUDA_TRY(cudaMemsetAsync(s->d_stats, 0, 11 * n * sizeof(double), s->ctx->stream));
+  CUDA_TRY(dalloc(s, &s->d_stats, 22 * n * sizeof(double)));
+  CUDA_TRY(cudaMemsetAsync(s->d_stats, 0, 22 * n * sizeof(double), s->ctx->stream));
   return FSLBM_OK;
 }
 
 extern "C" int fslbm_stats_sample(fslbm_solve* s) {
   if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "stats_sample: null solve");
+  NvtxRange range("fslbm_stats_sample");
   CUDA_TRY(cudaSetDevice(s->ctx->device));
   if (int r = ensure_stats(s)) return r;
   const size_t n = size_t(s->ly) * (s->L + 2 * s->d2);
@@ -1123,10 +1125,11 @@ extern "C" int fslbm_stats_sample(fslbm_solve* s) {
   // reset policy (FSLBM.cu:683-690)
   if (s->prm.delta == 0) {
     s->cnt = 0; s->cnt2 = 0;
-    CUDA_TRY(cudaMemsetAsync(s->d_stats, 0, 11 * n * sizeof(double), st));
+    CUDA_TRY(cudaMemsetAsync(s->d_stats, 0, 22 * n * sizeof(double), st));
   } else if (s->prm.delta == 1) {
     s->cnt2 = 0;
     CUDA_TRY(cudaMemsetAsync(s->d_stats + 4 * n, 0, 7 * n * sizeof(double), st));
+    CUDA_TRY(cudaMemsetAsync(s->d_stats + 15 * n, 0, 7 * n * sizeof(double), st));
   }
   s->cnt += 1; s->cnt2 += 1;                                   // FSLBM.cu:715
   const double pin = s->dtype != FSLBM_F64 ? double(float(s->prm.pin)) : s->prm.pin;
@@ -1140,11 +1143,14 @@ extern "C" int fslbm_stats_get(fslbm_solve* s, double* out, int* cnt, int* cnt2)
   CUDA_TRY(cudaSetDevice(s->ctx->device));
   if (int r = ensure_stats(s)) return r;
   const size_t n = size_t(s->ly) * (s->L + 2 * s->d2);
-  CUDA_TRY(cudaMemcpyAsync(out, s->d_stats, 11 * n * sizeof(double), cudaMemcpyDeviceToHost,
+  std::vector<double> acc(22 * n);
+  CUDA_TRY(cudaMemcpyAsync(acc.data(), s->d_stats, 22 * n * sizeof(double), cudaMemcpyDeviceToHost,
                            s->ctx->stream));
   CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
-  for (size_t k = 0; k < 4 * n; ++k) out[k] = s->cnt ? out[k] / double(s->cnt) : 0.0;
-  for (size_t k = 4 * n; k < 11 * n; ++k) out[k] = s->cnt2 ? out[k] / double(s->cnt2) : 0.0;
+  for (size_t k = 0; k < 11 * n; ++k) {
+    const int c = k < 4 * n ? s->cnt : s->cnt2;
+    out[k] = c ? (acc[k] + acc[11 * n + k]) / double(c) : 0.0;   // compensated sum / count
+  }
   if (cnt) *cnt = s->cnt;
   if (cnt2) *cnt2 = s->cnt2;
   return FSLBM_OK;
@@ -1155,7 +1161,7 @@ extern "C" int fslbm_stats_set(fslbm_solve* s, const double* means, int cnt, int
   CUDA_TRY(cudaSetDevice(s->ctx->device));
   if (int r = ensure_stats(s)) return r;
   const size_t n = size_t(s->ly) * (s->L + 2 * s->d2);
-  std::vector<double> sums(11 * n);
+  std::vector<double> sums(22 * n, 0.0);                                      // compensations 0
   for (size_t k = 0; k < 4 * n; ++k) sums[k] = means[k] * double(cnt);        // FSLBM.cu:453-456
   for (size_t k = 4 * n; k < 11 * n; ++k) sums[k] = means[k] * double(cnt2);  // FSLBM.cu:457-463
   CUDA_TRY(cudaMemcpyAsync(s->d_stats, sums.data(), sums.size() * sizeof(double),
@@ -1166,11 +1172,12 @@ extern "C" int fslbm_stats_set(fslbm_solve* s, const double* means, int cnt, int
 
 extern "C" int fslbm_profile_sample(fslbm_solve* s) {
   if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "profile_sample: null solve");
+  NvtxRange range("fslbm_profile_sample");
   CUDA_TRY(cudaSetDevice(s->ctx->device));
   const size_t n = size_t(s->lxp) * s->ly;
   if (!s->d_prof) {
-    CUDA_TRY(dalloc(s, &s->d_prof, 10 * n * sizeof(double)));
-    CUDA_TRY(cudaMemsetAsync(s->d_prof, 0, 10 * n * sizeof(double), s->ctx->stream));
+    CUDA_TRY(dalloc(s, &s->d_prof, 20 * n * sizeof(double)));
+    CUDA_TRY(cudaMemsetAsync(s->d_prof, 0, 20 * n * sizeof(double), s->ctx->stream));
   }
   CUDA_TRY(launch_profile(s->dtype, s->state[s->cur], s->lxp, s->ly, s->L, s->d_prof, s->ctx->stream));
   s->prof_n += 1;
@@ -1181,7 +1188,7 @@ extern "C" int fslbm_profile_get(fslbm_solve* s, double* sums, int64_t* nsamples
   if (!s || !sums) return fslbm_set_error(FSLBM_ERR_ARG, "profile_get: null argument");
   CUDA_TRY(cudaSetDevice(s->ctx->device));
   const size_t n = size_t(s->lxp) * s->ly;
-  std::vector<double> buf(10 * n, 0.0);
+  std::vector<double> buf(20 * n, 0.0);
   if (s->d_prof) {
     CUDA_TRY(cudaMemcpyAsync(buf.data(), s->d_prof, buf.size() * sizeof(double),
                              cudaMemcpyDeviceToHost, s->ctx->stream));
@@ -1190,7 +1197,8 @@ extern "C" int fslbm_profile_get(fslbm_solve* s, double* sums, int64_t* nsamples
   for (int k = 0; k < 10; ++k)
     for (int y = 0; y < s->ly; ++y)
       for (int x = 0; x < s->lx; ++x)
-        sums[(size_t(k) * s->ly + y) * s->lx + x] = buf[(size_t(k) * s->ly + y) * s->lxp + x];
+        sums[(size_t(k) * s->ly + y) * s->lx + x] =
+            buf[(size_t(k) * s->ly + y) * s->lxp + x] + buf[(size_t(10 + k) * s->ly + y) * s->lxp + x];
   if (nsamples) *nsamples = s->prof_n;
   return FSLBM_OK;
 }
@@ -1199,7 +1207,7 @@ extern "C" int fslbm_profile_reset(fslbm_solve* s) {
   if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "profile_reset: null solve");
   if (s->d_prof) {
     CUDA_TRY(cudaSetDevice(s->ctx->device));
-    CUDA_TRY(cudaMemsetAsync(s->d_prof, 0, 10 * size_t(s->lxp) * s->ly * sizeof(double), s->ctx->stream));
+    CUDA_TRY(cudaMemsetAsync(s->d_prof, 0, 20 * size_t(s->lxp) * s->ly * sizeof(double), s->ctx->stream));
   }
   s->prof_n = 0;
   return FSLBM_OK;
@@ -1511,6 +1519,7 @@ extern "C" int fslbm_batch_step(fslbm_batch* b, int64_t nsteps, int use_graph) {
   if (nsteps < 0) return fslbm_set_error(FSLBM_ERR_ARG, "batch_step: negative step count");
   for (fslbm_solve* s : b->members)
     if (!s->fields_set) return fslbm_set_error(FSLBM_ERR_STATE, "batch_step: a member has no fields");
+  NvtxRange range("fslbm_batch_step");
   CUDA_TRY(cudaSetDevice(b->ctx->device));
   cudaStream_t st = b->ctx->stream;
   // steps each member actually takes (a member stops at its stop step)
@@ -1707,18 +1716,28 @@ extern "C" int fslbm_batch_autotune(fslbm_batch* b, int trial_steps, const char*
     cur_ms = best.ms;
     table[order[oi].second] = best;
   }
-  // restore every member and free every snapshot even when a step fails; keep the first error
+  // Restore every member and free every snapshot even when a step fails; keep the first error.
+  // A member's host-side counters are put back only with its device state, counters and gauge;
+  // a member whose copies could not be queued is marked as having no fields, so it refuses to
+  // step (FSLBM_ERR_STATE) until its fields are set again, instead of stepping a state that
+  // disagrees with its counters.
   b->stop = stops;
   cudaError_t re = cudaStreamSynchronize(st);
+  int unrestored = 0;
   for (int i = 0; i < n; ++i) {
     fslbm_solve* s = b->members[i];
     Snap& q = snap[i];
     if (!q.state) continue;
-    s->steps = q.steps; s->cur = q.cur; s->launches = q.launches; s->drained = q.drained;
-    if (!re) re = cudaMemcpyAsync(s->state[s->cur], q.state, 4 * field_stride(s) * s->es,
+    if (!re) re = cudaMemcpyAsync(s->state[q.cur], q.state, 4 * field_stride(s) * s->es,
                                   cudaMemcpyDeviceToDevice, st);
     if (!re) re = cudaMemcpyAsync(s->d_counters, &q.c, sizeof q.c, cudaMemcpyHostToDevice, st);
     if (!re) re = cudaMemcpyAsync(s->d_gauge, &q.gauge, sizeof q.gauge, cudaMemcpyHostToDevice, st);
+    if (!re) {
+      s->steps = q.steps; s->cur = q.cur; s->launches = q.launches; s->drained = q.drained;
+    } else {
+      s->fields_set = false;
+      ++unrestored;
+    }
     ctx_free(b->ctx, q.state);                     // stream-ordered: after the copy
   }
   if (!re) re = cudaMemsetAsync(b->d_tickets + 2, 0, sizeof(unsigned), st);
@@ -1726,8 +1745,9 @@ extern "C" int fslbm_batch_autotune(fslbm_batch* b, int trial_steps, const char*
   if (!re) re = se;
   b->h_items.clear();
   if (rc) return rc;
-  if (re) return fslbm_set_error(FSLBM_ERR_CUDA, "batch_autotune: restoring the members: %s",
-                                 cudaGetErrorString(re));
+  if (re) return fslbm_set_error(FSLBM_ERR_CUDA, "batch_autotune: restoring the members: %s (%d "
+                                 "members not restored: their fields must be set again)",
+                                 cudaGetErrorString(re), unrestored);
   if (path && !write_tiling(path, table))
     return fslbm_set_error(FSLBM_ERR_IO, "batch_autotune: cannot write %s", path);
   return FSLBM_OK;

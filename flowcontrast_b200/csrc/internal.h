@@ -6,6 +6,19 @@
 #include "../../include/fslbm.h"
 #include "common.h"
 #include "noise.h"
+#include <nvtx3/nvToolsExt.h>
+
+namespace fslbm {
+// NVTX range over a host-side scope (step enqueues, batch launches, statistics, server rounds),
+// so a timeline tool shows which API call issued which kernels. NVTX v3 is header-only and does
+// nothing unless a tool is attached.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+}  // namespace fslbm
 
 namespace fslbm {
 

@@ -663,10 +663,23 @@ cudaError_t launch_check(int dtype, const void* state, size_t n_per_field, doubl
 }
 
 // ------------------------------------------------------------------------------------------
+// Compensated FP64 accumulation (Neumaier's variant of Kahan summation): *s holds the running
+// sum, *c the rounding error the additions lost; the accumulated value is *s + *c. Long runs add
+// thousands of samples into one accumulator, where plain FP64 sums lose about one rounding per
+// addition relative to the total.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void comp_add(double* s, double* c, double x) {
+  const double a = *s, t = a + x;
+  *c += fabs(a) >= fabs(x) ? (a - t) + x : (x - t) + a;
+  *s = t;
+}
+
+// ------------------------------------------------------------------------------------------
 // reference plane statistics (FSLBM.cu:715-748) on the YZ plane x = xs of the reference
 // layout: rows y, columns z_ref in [0, L+2*d2); buffer planes are the wrapped core planes with
 // p +- pin on non-wall cells, in the storage type's arithmetic as the reference's bcond does.
-// acc: 11 arrays of ly*(L+2*d2) doubles; cnt is the mean count including this sample.
+// acc: 11 arrays of ly*(L+2*d2) running sums, then 11 arrays of their compensations; cnt is
+// the mean count including this sample. The deviation is taken from the compensated mean.
 // ------------------------------------------------------------------------------------------
 template <class TS>
 __global__ void plane_stats_kernel(const TS* s, const uint8_t* mask, int planes, int lxp, int ly,
@@ -675,6 +688,7 @@ __global__ void plane_stats_kernel(const TS* s, const uint8_t* mask, int planes,
   const size_t n = size_t(ly) * Lr, FS = size_t(lxp) * ly * L;
   using TA = typename ArithOf<TS>::type;
   const TA pin = TA(pin_d);
+  double* cmp = acc + 11 * n;
   for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n;
        k += size_t(gridDim.x) * blockDim.x) {
     const int y = int(k % ly), zr = int(k / ly);
@@ -686,21 +700,19 @@ __global__ void plane_stats_kernel(const TS* s, const uint8_t* mask, int planes,
       if (jump == 1) p = TA(p + pin);
       else if (jump == -1) p = TA(p - pin);
     }
-    const double qp = double(p), qu = to_d(s[FS + o]), qv = to_d(s[2 * FS + o]),
-                 qw = to_d(s[3 * FS + o]);
+    const double q[4] = {double(p), to_d(s[FS + o]), to_d(s[2 * FS + o]), to_d(s[3 * FS + o])};
     const double c = double(cnt);
-    double* a = acc;
-    a[k] += qp;          const double dd1 = a[k] / c - qp;
-    a[n + k] += qu;      const double dd2 = a[n + k] / c - qu;
-    a[2 * n + k] += qv;  const double dd3 = a[2 * n + k] / c - qv;
-    a[3 * n + k] += qw;  const double dd4 = a[3 * n + k] / c - qw;
-    a[4 * n + k] += fabs(dd1);
-    a[5 * n + k] += fabs(dd2);
-    a[6 * n + k] += fabs(dd3);
-    a[7 * n + k] += fabs(dd4);
-    a[8 * n + k] += dd2 * dd3;
-    a[9 * n + k] += dd2 * dd4;
-    a[10 * n + k] += dd4 * dd3;
+    double dd[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {           // running mean including this sample, deviation
+      comp_add(&acc[f * n + k], &cmp[f * n + k], q[f]);
+      dd[f] = (acc[f * n + k] + cmp[f * n + k]) / c - q[f];
+    }
+#pragma unroll
+    for (int f = 0; f < 4; ++f) comp_add(&acc[(4 + f) * n + k], &cmp[(4 + f) * n + k], fabs(dd[f]));
+    comp_add(&acc[8 * n + k], &cmp[8 * n + k], dd[1] * dd[2]);
+    comp_add(&acc[9 * n + k], &cmp[9 * n + k], dd[1] * dd[3]);
+    comp_add(&acc[10 * n + k], &cmp[10 * n + k], dd[3] * dd[2]);
   }
 }
 
@@ -719,8 +731,11 @@ cudaError_t launch_plane_stats(int dtype, const void* state, const uint8_t* mask
 }
 
 // ------------------------------------------------------------------------------------------
-// full-volume profile statistics: per column (x,y), sums over z of
-// p,u,v,w,uu,vv,ww,uv,uw,vw (FP64). Block = 32 columns x 8 z-lanes; atomics per block.
+// full-volume profile statistics: per column (x,y), sums over z of p,u,v,w,uu,vv,ww,uv,uw,vw
+// (FP64), added to the accumulators with compensation. Block = 32 columns x 8 z-lanes over
+// every plane; the lanes' partial sums are combined in a fixed order, so a sample's sums and
+// hence the accumulated profile do not depend on scheduling. acc: 10 arrays of lxp*ly sums,
+// then 10 arrays of their compensations.
 // ------------------------------------------------------------------------------------------
 template <class TS>
 __global__ void profile_kernel(const TS* s, int lxp, int ly, int L, double* acc) {
@@ -730,7 +745,7 @@ __global__ void profile_kernel(const TS* s, int lxp, int ly, int L, double* acc)
   const size_t FS = size_t(lxp) * ly * L, cs = size_t(lxp) * ly;
   double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (x < lxp) {
-    for (int z = blockIdx.z * 8 + tz; z < L; z += gridDim.z * 8) {
+    for (int z = tz; z < L; z += 8) {
       const size_t o = (size_t(z) * ly + y) * lxp + x;
       const double p = to_d(s[o]), u = to_d(s[FS + o]), vv = to_d(s[2 * FS + o]),
                    w = to_d(s[3 * FS + o]);
@@ -742,19 +757,19 @@ __global__ void profile_kernel(const TS* s, int lxp, int ly, int L, double* acc)
   for (int k = 0; k < 10; ++k) sh[k][tz][tx] = v[k];
   __syncthreads();
   if (tz == 0 && x < lxp) {
+    const size_t i = size_t(y) * lxp + x;
 #pragma unroll
     for (int k = 0; k < 10; ++k) {
       double t = 0;
       for (int j = 0; j < 8; ++j) t += sh[k][j][tx];
-      atomicAdd(&acc[k * cs + size_t(y) * lxp + x], t);
+      comp_add(&acc[k * cs + i], &acc[(10 + k) * cs + i], t);
     }
   }
 }
 
 cudaError_t launch_profile(int dtype, const void* state, int lxp, int ly, int L, double* acc,
                            cudaStream_t st) {
-  dim3 grid((lxp + 31) / 32, ly, (L + 63) / 64 < 8 ? (L + 63) / 64 : 8);
-  if (grid.z < 1) grid.z = 1;
+  dim3 grid((lxp + 31) / 32, ly, 1);
   if (dtype == FSLBM_F32) profile_kernel<float><<<grid, 256, 0, st>>>((const float*)state, lxp, ly, L, acc);
   else if (dtype == FSLBM_F64) profile_kernel<double><<<grid, 256, 0, st>>>((const double*)state, lxp, ly, L, acc);
   else if (dtype == FSLBM_F16) profile_kernel<__half><<<grid, 256, 0, st>>>((const __half*)state, lxp, ly, L, acc);

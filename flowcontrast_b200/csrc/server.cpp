@@ -20,6 +20,8 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/fslbm.h"
 
 int fslbm_set_error(int code, const char* fmt, ...);
@@ -259,6 +261,10 @@ void run(fslbm_server* S) {
       continue;
     }
     const auto tg = Clock::now();
+    struct RoundRange {              // NVTX range over the round (header-only NVTX v3)
+      RoundRange() { nvtxRangePushA("fslbm_server_round"); }
+      ~RoundRange() { nvtxRangePop(); }
+    } range;
     const std::vector<ReqPtr> round = round_set(S);
     for (const ReqPtr& r : round) r->in_round = true;
     const int rg = regroup(S, round);

@@ -189,9 +189,10 @@ int fslbm_solve_get_plane(fslbm_solve* s, int kind, int comp, float* out);
 
 /* ---- statistics ---- */
 /* Reference plane statistics (FSLBM.cu:683-768) on the YZ plane x=lx/2 of the reference layout,
- * accumulated on the device in FP64. fslbm_stats_sample applies the `delta` reset policy of the
+ * accumulated on the device in FP64 with compensated (Neumaier) sums, so long runs of samples
+ * lose no precision to rounding. fslbm_stats_sample applies the `delta` reset policy of the
  * current parameters, then adds one sample (cnt and cnt2 are incremented first, as in the
- * reference). Outputs are 11 arrays of ly*(lz+2*d2) doubles in the order
+ * reference). The "RMS" sums are of |deviation|, as the reference's abs() of a double. Outputs are 11 arrays of ly*(lz+2*d2) doubles in the order
  * _p,_ux,_uy,_uz (sums / cnt), _p2,_ux2,_uy2,_uz2,_uxy2,_uxz2,_uyz2 (sums / cnt2). */
 int fslbm_stats_sample(fslbm_solve* s);
 int fslbm_stats_get(fslbm_solve* s, double* out, int* cnt, int* cnt2);
@@ -199,7 +200,8 @@ int fslbm_stats_get(fslbm_solve* s, double* out, int* cnt, int* cnt2);
  * the means are multiplied back by their counts. */
 int fslbm_stats_set(fslbm_solve* s, const double* means, int cnt, int cnt2);
 /* Full-volume profile statistics (addition): per cross-section cell, FP64 sums over z and over
- * samples of p,u,v,w,uu,vv,ww,uv,uw,vw (10 arrays of lx*ly). */
+ * samples of p,u,v,w,uu,vv,ww,uv,uw,vw (10 arrays of lx*ly); samples are added with
+ * compensated sums in a fixed order, so the result does not depend on scheduling. */
 int fslbm_profile_sample(fslbm_solve* s);
 int fslbm_profile_get(fslbm_solve* s, double* sums, int64_t* nsamples);
 int fslbm_profile_reset(fslbm_solve* s);
@@ -232,7 +234,9 @@ int fslbm_batch_load_tiling(fslbm_batch* b, const char* path);
 /* Autotuner: times each size class's candidate tilings (chunks 16..256, both warp shapes) on the
  * batch itself, trial_steps steps per candidate, keeps the fastest per class, restores every
  * member's fields, step count, monitor log and gauge, and writes the table to `path` (JSON) if
- * not NULL. Needs members on the batched kernel (FP32 or FP16 storage, d1 = 2). */
+ * not NULL. Needs members on the batched kernel (FP32 or FP16 storage, d1 = 2). If a member's
+ * state cannot be restored (a CUDA error), the call fails and that member refuses to step
+ * (FSLBM_ERR_STATE) until its fields are set again. */
 int fslbm_batch_autotune(fslbm_batch* b, int trial_steps, const char* path);
 
 /* ---- served solves: a request loop with continuous batching (no reference counterpart) ----

@@ -100,3 +100,126 @@ def test_cli_restart_continues(built, tmp_path):
     assert np.linalg.norm(u_a - u_b) <= 1e-5 * np.linalg.norm(u_a)
     # statistics continue from the backup: the same sample counts as the straight run
     assert lines(b, "_av.txt") == lines(a, "_av.txt")
+
+
+STAT_FILES = ("_p.txt", "_ux.txt", "_uy.txt", "_uz.txt", "_p2.txt", "_ux2.txt", "_uy2.txt",
+              "_uz2.txt", "_uxy2.txt", "_uxz2.txt", "_uyz2.txt")
+
+
+def test_cli_live_param_reload_and_statistics(built, ctx, tmp_path):
+    """Live param.txt reload (FSLBM.cu:667-690) with the delta reset policy, end to end.
+
+    param.txt is a named pipe, so each of the CLI's reads (at start-up and before the
+    statistics of every 500-step dump) blocks until this test hands it the next parameter set:
+    start delta 2, nu 0.02; dump 500: nu 0.03 (delta 2); dump 1000: delta 1 (the fluctuation
+    sums restart); dump 1500: delta 0 (everything restarts); dump 2000: delta 2, tblend 0.8.
+    After each dump the statistics files and _av.txt are captured and compared with the same
+    schedule run through the library (fslbm_solve_set_params, then fslbm_stats_sample), whose
+    statistics the device-statistics tests pin to the oracle: the counts follow the policy
+    and every value equals the library's "%e" text. The printed dtddy follows the new nu.
+    """
+    import threading
+
+    fb = built
+    d = str(tmp_path)
+    mask = write_inputs(fb, d)
+    base = fb.read_param_txt(os.path.join(d, "param.txt"))
+    os.remove(os.path.join(d, "param.txt"))
+    sched = [dict(nu=0.02, delta=2), dict(nu=0.03, delta=2), dict(nu=0.03, delta=1),
+             dict(nu=0.03, delta=0), dict(nu=0.03, delta=2, tblend=0.8)]
+    texts = []
+    for k, upd in enumerate(sched):
+        p = fb.Params.from_buffer_copy(base)
+        for key, val in upd.items():
+            setattr(p, key, val)
+        path = os.path.join(d, f"param{k}.tmp")
+        fb.write_param_txt(path, p)
+        texts.append(open(path).read())
+    fifo = os.path.join(d, "param.txt")
+    os.mkfifo(fifo)
+    proc = subprocess.Popen([CLI, *SMALL, "--steps", "2000"], cwd=d, stdout=subprocess.PIPE,
+                            stderr=subprocess.PIPE, text=True)
+    snaps = []
+
+    def snapshot():
+        snaps.append({n: lines(d, n) for n in STAT_FILES + ("_av.txt",)})
+
+    def qp_lines():
+        try:
+            with open(os.path.join(d, "qp.txt")) as fh:
+                return fh.read().count("\n")
+        except OSError:
+            return 0
+
+    def feeder():
+        # Hands texts[k] to the k-th read (start-up, then the dumps at steps 500k). The next
+        # open waits until qp.txt holds the monitor record of step 500k + 50, which the CLI
+        # writes after it closed param.txt, so two parameter sets never share one read.
+        import errno
+        import time
+        for k, text in enumerate(texts):
+            fd = None
+            t0 = time.time()
+            while fd is None and proc.poll() is None and time.time() - t0 < 300:
+                try:
+                    fd = os.open(fifo, os.O_WRONLY | os.O_NONBLOCK)
+                except OSError as e:
+                    if e.errno != errno.ENXIO:
+                        raise
+                    time.sleep(0.001)
+            if fd is None:
+                return
+            if k >= 2:
+                snapshot()                # the previous dump's files are complete
+            os.set_blocking(fd, True)
+            os.write(fd, text.encode())
+            os.close(fd)
+            if k + 1 < len(texts):
+                while qp_lines() < 10 * k + 1 and proc.poll() is None and time.time() - t0 < 300:
+                    time.sleep(0.001)
+
+    th = threading.Thread(target=feeder, daemon=True)
+    th.start()
+    try:
+        out, err = proc.communicate(timeout=600)
+    finally:
+        if proc.poll() is None:
+            proc.kill()
+    th.join(timeout=10)
+    assert proc.returncode == 0, err
+    snapshot()
+    assert len(snaps) == 4
+    assert [s["_av.txt"] for s in snaps] == [["1 1"], ["2 1"], ["1 1"], ["2 2"]]
+    dtddy = [float(l.split("dtddy: ")[1].split(",")[0]) for l in out.splitlines()
+             if l.startswith("time step:")]
+    assert len(dtddy) == 40
+    assert abs(dtddy[9] - (0.02 - 0.16666666)) < 1e-6 and abs(dtddy[10] - (0.03 - 0.16666666)) < 1e-6
+
+    # the same schedule through the library
+    core = fb.ref_mask_to_core(mask, 10)
+    lz, ly, lx = mask.shape
+    dom = fb.make_domain(lx, ly, lz - 20, mask=core, radius=10.0, buffer_depth=10)
+    prms = []
+    for k in range(len(texts)):
+        p = fb.read_param_txt(os.path.join(d, f"param{k}.tmp"))
+        p.monitor_every = 50
+        prms.append(p)
+    s = fb.Solve(ctx, dom, prms[0], fb.F32)
+    f = np.zeros((4, lz, ly, lx), np.float32)
+    z = np.arange(lz, dtype=np.float32)
+    f[0] = (np.float32(np.float32(0.003) * (np.float32(lz - 10) - z)) / np.float32(lz - 20))[:, None, None]
+    s.set_fields_ref(f)
+    try:
+        for k in range(4):
+            s.step(500)
+            s.set_params(prms[k + 1])
+            s.stats_sample()
+            means, cnt, cnt2 = s.stats_get()
+            assert snaps[k]["_av.txt"] == [f"{cnt} {cnt2}"]
+            for j, name in enumerate(STAT_FILES):
+                got = [float(v) for v in snaps[k][name]]
+                assert got == [float(f"{v:e}") for v in means[j]], (k, name)
+        # the fluctuation statistics are not trivially zero
+        assert np.abs(means[4:8]).max() > 0
+    finally:
+        s.close()

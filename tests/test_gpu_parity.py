@@ -206,3 +206,24 @@ def test_laminar_poiseuille_profile(built, ctx):
     assert abs(beta - g / (4 * nu)) / (g / (4 * nu)) < 0.02, (beta, g / (4 * nu))
     assert 13.0 < r_eff < 17.0, r_eff
     assert np.abs(b[3] - a[3]).max() / alpha < 1e-3
+
+
+def test_production_cross_section_slab_fp32(built, ctx):
+    """The production pipe's cross-section (128 x 128, R = 63 centred at (63.5, 63.5): every
+    tile holds fluid) on a 64-plane slab, the benchmark's parameters (order-4 corrector, tblend
+    0.02, nu 0.0111, body force), 40 steps with the monitor and gauge every 20: the FP32 kernel
+    as the benchmark launches it (every tile, several streamwise chunks per tile in both march
+    directions) against the FP64 oracle within 1e-5."""
+    lx = ly = 128
+    L, R = 64, 63.0
+    m2 = circle_mask(lx, ly, R, 63.5, 63.5)
+    dom = built.make_domain(lx, ly, L, radius=R, cx=63.5, cy=63.5, buffer_depth=10)
+    ub = 5300.0 * 0.0111 / (2 * R)
+    g = 2 * (180.0 * 0.0111 / R) ** 2 / R
+    f = built.init_poiseuille(dom, 2 * ub, noise=1e-3, modes=4, mode_amp=0.05, seed=77)
+    prm = dict(tblend=0.02, pin=0.0, nu=0.0111, d1=2, blend=1.0, force=(0.0, 0.0, -g))
+    ref, _ = O.run_core(m2, L, f, prm, 40, monitor_every=20, radius=R)
+    got, log = run_gpu(built, ctx, dom, prm, built.F32, f, 40, monitor_every=20)
+    ep, eu, eps = errors(got, ref, m2)
+    assert len(log) == 2
+    assert eu <= 1e-5 and eps <= 1e-5, (ep, eu, eps)
