@@ -3,10 +3,20 @@
 // oracle. Built by oracle/Makefile into oracle/_ref/libfslbm_ref.so from the reference source
 // where it lies (the include path is given by the recipe); nothing of the reference is copied.
 //
-// The host loop restates FSLBM.cu:620-628: per step 38-style descending slab launches of
-// FSLBMcalc (grid (lx/8+1, ly/8+1, 1), block 8x8x8), (lz-d2) shiftback plane launches, then one
-// bcond. The gauge p2 is held at 0: the reference's bcond races when p2 != 0 (FSLBM.cu:295,303),
-// so golden runs stay below the first monitor step (50).
+// The host loop restates FSLBM.cu:620-628: per step descending slab launches of FSLBMcalc
+// (grid (lx/8+1, ly/8+1, 1), block 8x8x8), (lz-d2) shiftback plane launches, then one bcond
+// with the gauge p2 of the previous step's monitor (0 otherwise), and, every monitor_every
+// steps, the outlet mean of FSLBM.cu:630-647 that sets the next p2 (FP32 sums in index order
+// over the whole plane, l1 accumulated as in FSLBM.cu:587-591).
+//
+// Read modes. As shipped, the reference's slab launch reads planes (texture fetches) that the
+// same launch writes when blend != 0 (the corrector taps at z+2*d1 reach the shifted output
+// planes, FSLBM.cu:253,275), and bcond reads interior planes that other threads of the launch
+// shift by p2 (FSLBM.cu:295,300,303). Texture reads are not coherent with surface writes inside
+// a launch, so those results depend on scheduling. With race_free = 1 each FSLBMcalc slab loop
+// and each bcond samples a copy of the field taken just before it (every read sees the values
+// of the step's start, resp. of the swept field), which is the Jacobi semantics the oracle and
+// the solver implement; the kernels themselves run unchanged.
 #include "ref_shim.h"
 #define main fslbm_reference_main
 #include "FSLBM.cu"
@@ -16,31 +26,61 @@
 
 extern "C" {
 
+// How the reference's statistics resolve the unqualified abs() they apply to doubles
+// (FSLBM.cu:741-744): this function sits in the same translation unit as FSLBM.cu, after its
+// includes (FSLBM.cu:28-34), built by the same nvcc line, so abs here is found the way it is
+// found there. A floating-point abs returns |x|; the int overload would truncate |x| < 1 to 0.
+double ref_abs_probe(double x) { return abs(x); }
+
 // io: lx*ly*lz mask; prm: tblend, pin, nu, d1, blend; in/out: 4*lx*ly*lz floats (p,u,v,w
-// blocks). ms_out (optional): device time of the nsteps loop in milliseconds. Returns 0, a
-// negative argument error, or a positive cudaError_t.
-int ref_run(const unsigned char* io, int lx, int ly, int lz, int d2, const float* prm,
-            const float* in, float* out, int nsteps, float* ms_out, unsigned* oob_out) {
-  if (lx % 8 || ly % 8 || lx <= 0 || ly <= 0 || lz <= 2 * d2 || d2 < 1 || nsteps < 0) return -1;
-  const long n = long(lx) * ly * lz;
+// blocks). monitor_every: 0 = no monitor (p2 stays 0), else the reference's period (50).
+// race_free: 0 = the kernels read the live field, as shipped; 1 = snapshot reads (see above).
+// ms_out (optional): device time of the nsteps loop in milliseconds; oob_out (optional): writes
+// dropped outside the box; p2_out (optional): the p2 of each monitor. Returns 0, a negative
+// argument error, or a positive cudaError_t.
+int ref_run2(const unsigned char* io, int lx, int ly, int lz, int d2, const float* prm,
+             const float* in, float* out, int nsteps, int monitor_every, int race_free,
+             float* ms_out, unsigned* oob_out, float* p2_out) {
+  if (lx % 8 || ly % 8 || lx <= 0 || ly <= 0 || lz <= 2 * d2 || d2 < 1 || nsteps < 0 ||
+      monitor_every < 0)
+    return -1;
+  const long n = long(lx) * ly * lz, lxy = long(lx) * ly;
   float tblend = prm[0], pin = prm[1], nu = prm[2], blend = prm[4];
   int d1 = int(prm[3]);
   float dtddy = (nu - 0.16666666f);                       // FSLBM.cu:599
-  std::vector<float4> h(n);
+  float l1 = 0.0f;                                        // FSLBM.cu:587-591
+  for (long i = 0; i < n; ++i)
+    if (io[i] == 1) l1 = l1 + 1.0f / float(2 * d2);
+  const float l2 = l1;
+  std::vector<float4> h(n), plane(lxy);
   for (long i = 0; i < n; ++i) h[i] = make_float4(in[i], in[n + i], in[2 * n + i], in[3 * n + i]);
-  float4* dfield = nullptr; char* dio = nullptr;
+  float4 *dfield = nullptr, *snap = nullptr;
+  char* dio = nullptr;
   cudaError_t e = cudaMalloc(&dfield, n * sizeof(float4));
   if (e) return int(e);
   e = cudaMalloc(&dio, n);
-  if (e) { cudaFree(dfield); return int(e); }
+  if (!e && race_free) e = cudaMalloc(&snap, n * sizeof(float4));
+  if (e) { cudaFree(dfield); cudaFree(dio); return int(e); }
   cudaMemcpy(dfield, h.data(), n * sizeof(float4), cudaMemcpyHostToDevice);
   cudaMemcpy(dio, io, n, cudaMemcpyHostToDevice);
   unsigned zero = 0;
+  const float4* live = dfield;
   cudaMemcpyToSymbol(ref_field, &dfield, sizeof(dfield));
+  cudaMemcpyToSymbol(ref_tex_src, &live, sizeof(live));
   cudaMemcpyToSymbol(ref_lx, &lx, sizeof(int));
   cudaMemcpyToSymbol(ref_ly, &ly, sizeof(int));
   cudaMemcpyToSymbol(ref_lz, &lz, sizeof(int));
   cudaMemcpyToSymbol(ref_oob_writes, &zero, sizeof(unsigned));
+  // race-free mode: texture fetches of the next launches read a copy of the current field
+  auto sample_copy = [&]() {
+    if (!race_free) return;
+    cudaMemcpy(snap, dfield, n * sizeof(float4), cudaMemcpyDeviceToDevice);
+    const float4* src = snap;
+    cudaMemcpyToSymbol(ref_tex_src, &src, sizeof(src));
+  };
+  auto sample_live = [&]() {
+    if (race_free) cudaMemcpyToSymbol(ref_tex_src, &live, sizeof(live));
+  };
 
   dim3 blocks2D(8, 8), grid2D(lx / 8 + 1, ly / 8 + 1);
   dim3 blocks3D(8, 8, 8), grid3D(lx / 8 + 1, ly / 8 + 1, lz / 8 + 1);
@@ -49,16 +89,28 @@ int ref_run(const unsigned char* io, int lx, int ly, int lz, int d2, const float
   cudaEventCreate(&e0); cudaEventCreate(&e1);
   cudaEventRecord(e0);
   float p2 = 0.0f;
-  for (int c = 1; c <= nsteps; ++c) {
+  int nmon = 0;
+  for (int c = 1; c <= nsteps && !e; ++c) {
+    sample_copy();
     for (int k = (lz - 1) - d2; k >= d2; k -= bdz)
       FSLBMcalc<<<grid3D1, blocks3D1>>>(dio, lx, ly, lz, dtddy, pin, nu, d2, k, tblend, d1,
                                         1.0 / float(d1 * d1), blend);
+    sample_live();
     for (int k = 0; k < (lz - d2); k++) shiftback<<<grid2D, blocks2D>>>(lx, ly, lz, d2, k);
+    sample_copy();
     bcond<<<grid3D, blocks3D>>>(dio, lx, ly, lz, d2, pin, p2);
     p2 = 0.0f;
+    sample_live();
+    if (monitor_every > 0 && c % monitor_every == 0) {   // FSLBM.cu:630-647 (outlet p mean)
+      e = cudaMemcpy(plane.data(), dfield + lxy * (lz - d2), lxy * sizeof(float4), cudaMemcpyDeviceToHost);
+      for (long i = 0; i < lxy; i++) p2 += plane[i].x;
+      p2 = p2 / l2;
+      if (p2_out) p2_out[nmon] = p2;
+      ++nmon;
+    }
   }
   cudaEventRecord(e1);
-  e = cudaEventSynchronize(e1);
+  if (!e) e = cudaEventSynchronize(e1);
   if (!e) e = cudaGetLastError();
   float ms = 0.f;
   cudaEventElapsedTime(&ms, e0, e1);
@@ -74,7 +126,14 @@ int ref_run(const unsigned char* io, int lx, int ly, int lz, int d2, const float
   }
   cudaEventDestroy(e0); cudaEventDestroy(e1);
   cudaFree(dfield); cudaFree(dio);
+  if (snap) cudaFree(snap);
   return int(e);
+}
+
+// The reference as shipped (live reads), without monitor.
+int ref_run(const unsigned char* io, int lx, int ly, int lz, int d2, const float* prm,
+            const float* in, float* out, int nsteps, float* ms_out, unsigned* oob_out) {
+  return ref_run2(io, lx, ly, lz, d2, prm, in, out, nsteps, 0, 0, ms_out, oob_out, nullptr);
 }
 
 }  // extern "C"

@@ -5,7 +5,9 @@
 // cudaBindTextureToArray, cudaBindSurfaceToArray), which FSLBM.cu:39-40 and :542-543 use. This
 // header emulates them over one plain float4 array in global memory:
 //   tex3D(ref, x, y, z)        point sampling at floor(coord), clamp addressing (the defaults of
-//                              an unnormalised texture reference)
+//                              an unnormalised texture reference), from ref_tex_src: the live
+//                              field, or (race-free mode of the harness) a copy of it taken
+//                              before the launches that read it
 //   surf3Dwrite(v, ref, xb,y,z) store at x = xb / sizeof(float4); out-of-box writes are dropped
 //                              and counted (the reference's launches never make one)
 //   surf3Dread<T>(ref, xb,y,z) load at x = xb / sizeof(float4)
@@ -26,6 +28,7 @@ template <class T, int D> struct RefSurface {};
 template <class T, int D, cudaTextureReadMode M> struct RefTexture {};
 
 __device__ float4* ref_field;        // lx*ly*lz cells, idx = x + lx*(y + ly*z)
+__device__ const float4* ref_tex_src;  // what tex3D samples: ref_field or a snapshot of it
 __device__ int ref_lx, ref_ly, ref_lz;
 __device__ unsigned int ref_oob_writes;
 
@@ -36,7 +39,7 @@ __device__ __forceinline__ float4 tex3D(RefTexture<float4, 3, cudaReadModeElemen
   const int ix = ref_clamp(int(floorf(float(x))), ref_lx);
   const int iy = ref_clamp(int(floorf(float(y))), ref_ly);
   const int iz = ref_clamp(int(floorf(float(z))), ref_lz);
-  return ref_field[ix + long(ref_lx) * (iy + long(ref_ly) * iz)];
+  return ref_tex_src[ix + long(ref_lx) * (iy + long(ref_ly) * iz)];
 }
 
 __device__ __forceinline__ void surf3Dwrite(float4 v, RefSurface<void, 3>, int xb, int y, int z) {

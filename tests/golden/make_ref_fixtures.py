@@ -5,7 +5,10 @@ Runs on a machine with a GPU, after `make -C oracle ref` has built oracle/_ref/l
 case in ref_cases.CASES and each step count, it advances the seeded initial state and stores
 the non-wall cells of the resulting reference-layout fields as float32:
 
-    python tests/golden/make_ref_fixtures.py --out tests/golden
+    python tests/golden/make_ref_fixtures.py --out tests/golden [--only name,name]
+
+Cases with `race_free` run the kernels on snapshot reads and cases with `monitor` apply the
+reference's gauge (see ref_cases.py).
 
 With --time it also times the reference's step loop on the demo grid (pipe.m, 120x120x320)
 and on a 128x128x(512+20) pipe, and writes ref_kernel_timing.json (context numbers only).
@@ -31,40 +34,48 @@ def load():
     u8 = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
     f32 = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
     i = ctypes.c_int
-    lib.ref_run.argtypes = [u8, i, i, i, i, f32, f32, f32, i,
-                            ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint)]
+    lib.ref_run2.argtypes = [u8, i, i, i, i, f32, f32, f32, i, i, i,
+                             ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint), f32]
     return lib
 
 
-def run(lib, io, fields, prm, nsteps):
+def run(lib, io, fields, prm, nsteps, monitor=0, race_free=0):
+    """Returns (fields, device ms, p2 of each monitor)."""
     lz, ly, lx = io.shape
     p = np.array([prm["tblend"], prm["pin"], prm["nu"], prm["d1"], prm["blend"]], np.float32)
     src = np.ascontiguousarray(fields, np.float32)
     out = np.empty_like(src)
+    p2 = np.zeros(max(1, nsteps // monitor if monitor else 0), np.float32)
     ms, oob = ctypes.c_float(0), ctypes.c_uint(0)
-    rc = lib.ref_run(np.ascontiguousarray(io), lx, ly, lz, prm["d2"], p, src.ravel(), out.ravel(),
-                     nsteps, ctypes.byref(ms), ctypes.byref(oob))
+    rc = lib.ref_run2(np.ascontiguousarray(io), lx, ly, lz, prm["d2"], p, src.ravel(), out.ravel(),
+                      nsteps, monitor, race_free, ctypes.byref(ms), ctypes.byref(oob), p2)
     if rc != 0:
-        raise RuntimeError(f"ref_run failed: {rc}")
+        raise RuntimeError(f"ref_run2 failed: {rc}")
     if oob.value:
         raise RuntimeError(f"reference kernels wrote {oob.value} cells outside the box")
-    return out, ms.value
+    return out, ms.value, p2[:nsteps // monitor if monitor else 0]
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--time", action="store_true")
+    ap.add_argument("--only", default="", help="comma-separated case names (default: all)")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     lib = load()
+    only = [x for x in a.only.split(",") if x]
     for name, c in ref_cases.CASES.items():
+        if only and name not in only:
+            continue
         io, ref, prm = ref_cases.inputs(name)
         keep = ref_cases.nonwall_index(io)
         arrays = {}
         for n in c["steps"]:
-            out, _ = run(lib, io, ref, prm, n)
+            out, _, p2 = run(lib, io, ref, prm, n, c.get("monitor", 0), c.get("race_free", 0))
             arrays[f"step{n}"] = out.reshape(4, -1)[:, keep]
+            if len(p2):
+                arrays[f"p2_step{n}"] = p2
         np.savez_compressed(os.path.join(a.out, f"ref_{name}.npz"), **arrays)
         print(name, {k: v.shape for k, v in arrays.items()})
     if a.time:
@@ -78,7 +89,7 @@ def main():
             prm = dict(tblend=1.0, pin=0.003, nu=0.004006, d1=2, blend=0.0, d2=ref_cases.D)
             run(lib, io, f, prm, 3)                      # warm-up
             steps = 40
-            _, ms = run(lib, io, f, prm, steps)
+            _, ms, _ = run(lib, io, f, prm, steps)
             cells = io.size
             res[label] = dict(cells=int(cells), steps=steps, ms=ms,
                               mlups=cells * steps / (ms * 1e-3) / 1e6)

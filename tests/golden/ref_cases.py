@@ -8,6 +8,12 @@ across machines), so the fixture files hold only the reference's outputs.
 Initial state: stored streamwise velocity w = -u0 (1 - r^2/R^2) plus uniform noise on all
 velocity components and on p; wall cells are zero; buffer planes hold the bcond copies of
 the wrapped core planes with the +-pin pressure jump (FSLBM.cu:291-301).
+
+`monitor` is the monitor period of the run (0: none, so the gauge p2 stays 0; 50: the
+reference's, so step 51 subtracts the p2 of step 50, FSLBM.cu:628-647). `race_free` runs the
+reference's kernels on snapshot reads (each slab loop and bcond sample the field as it was
+before them), which removes their intra-launch read/write races when blend != 0 or p2 != 0
+and leaves the arithmetic as compiled; cases with blend 0 and no gauge run as shipped.
 """
 import numpy as np
 
@@ -26,6 +32,14 @@ CASES = {
     "d1_one": dict(lx0=12, l0=16, seed=13, u0=0.04, noise=0.004, pnoise=1e-3,
                    prm=dict(tblend=0.5, pin=0.002, nu=0.12, d1=1, blend=0.0),
                    steps=(1, 25)),
+    # the benchmark's setting: order-4 corrector (blend 1) in the paper's regime
+    "paper_blend1": dict(lx0=12, l0=24, seed=14, u0=0.3, noise=0.03, pnoise=2e-3,
+                         prm=dict(tblend=0.02, pin=0.0193, nu=0.0111, d1=2, blend=1.0),
+                         steps=(1, 40), race_free=1),
+    # order-4 corrector across the first monitor: step 51 applies the gauge p2 of step 50
+    "gauge_blend1": dict(lx0=12, l0=16, seed=15, u0=0.05, noise=0.005, pnoise=1e-3,
+                         prm=dict(tblend=0.6, pin=0.003, nu=0.02, d1=2, blend=1.0),
+                         steps=(50, 51, 56), monitor=50, race_free=1),
 }
 
 
