@@ -555,7 +555,8 @@ def run_served(args):
     import flowcontrast_b200 as fb
     from flowcontrast_b200 import build, workloads as wl
     build.build()
-    reqs = wl.request_stream(args.requests, rate=200.0)
+    f32_only = args.served_dtype == "f32"
+    reqs = wl.request_stream(args.requests, rate=200.0, mixed_fraction=0.0 if f32_only else 0.5)
     check = set(range(0, len(reqs), max(1, len(reqs) // 4)))     # requests checked afterwards
     srv = fb.Server(0, hbm_budget=int(150e9), quantum=50)
     # warm-up (kernel set-up and graph capture paths), not counted
@@ -631,10 +632,11 @@ def run_served(args):
     line = {"metric": "aggregate MLUPS and p50/p95/p99 latency, served solves", "value": work / span / 1e6,
             "unit": "MLUPS", "n_gpus": 1, "steps": len(reqs), "warmup": 4,
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32+f16", "data": "synthetic (seeded Poisson request stream)",
+            "dtype": "f32" if f32_only else "f32+f16", "data": "synthetic (seeded Poisson request stream)",
             "config": {"workload": f"{len(reqs)} requests, Poisson 200/s, cells log-uniform "
                                    "32^3..256x96x96, steps U[200,5000], Re log-uniform [50,5000], "
-                                   "FP32 or FP16 storage 50/50, budget 150 GB, quantum 50",
+                                   + ("FP32 storage only" if f32_only else "FP32 or FP16 storage 50/50")
+                                   + ", budget 150 GB, quantum 50",
                        "requests": len(reqs), "policy": "every resident request each round"},
             "latency_s": {"p50": _pct(lat, 50), "p95": _pct(lat, 95), "p99": _pct(lat, 99),
                           "max": max(lat) if lat else None},
@@ -718,6 +720,8 @@ def main():
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--workload", default="plain", choices=["plain", "ensemble", "served", "mixed"])
     ap.add_argument("--requests", type=int, default=1000, help="served workload: request count")
+    ap.add_argument("--served-dtype", default="mixed", choices=["mixed", "f32"],
+                    help="served workload: storage types of the requests (FP32/FP16 50/50, or FP32)")
     ap.add_argument("--tuning-out", default=None, help="ensemble workload: write the tuned tiling table here")
     args = ap.parse_args()
     if args.warmup < 3:
