@@ -32,7 +32,7 @@ def ref_plane(f, mask2d, L, d2, pin, xs, fp32):
     cells, formed in the storage type's arithmetic."""
     zr = np.arange(L + 2 * d2)
     zc = (zr - d2) % L
-    pl = f[:, zc, :, xs]                                       # (4, L + 2 d2, ly)
+    pl = f[:, zc][..., xs]                                     # (4, L + 2 d2, ly)
     jump = np.where(zr < d2, 1.0, np.where(zr >= d2 + L, -1.0, 0.0))[:, None]
     off = jump * (mask2d[:, xs] != 125)[None, :]
     if fp32:

@@ -9,7 +9,12 @@ oracle's monitor forms that p2 in FP64, the reference's harness in FP32 as the r
 Tolerance: relative L2 over non-wall cells of the reference layout, separately for u=(u,v,w)
 and for p scaled by |p| + 1.5|u|^2: 2e-6 (both sides compute in FP32 with different operation
 order; FP32-vs-FP64 drift of the method itself is ~1e-6 over 40 steps on these cases). The
-gauges agree to 1e-5 relative (FP32 sums of about 100 values against FP64 ones).
+gauges agree to 1e-4 relative: the reference forms the cell count l1 by adding 1/(2 d2) in FP32
+once per buffer cell (FSLBM.cu:589-591), about 2300 additions of an inexact 0.05 here, which
+leaves it about 2e-5 off the exact count the oracle and the solver use. A gauge shifts p by
+the same amount on every non-wall cell, and later steps keep a uniform shift of p uniform (the
+weights sum to one and the wall rule copies the centre's p) without touching u, so p is
+compared after removing the difference of the applied gauges (gauge_offset).
 """
 import ctypes
 import os
@@ -23,7 +28,7 @@ import ref_cases as RC
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 TOL = 2e-6
-GAUGE_TOL = 1e-5
+GAUGE_TOL = 1e-4
 
 
 def load(name):
@@ -32,6 +37,17 @@ def load(name):
         pytest.fail(f"golden fixture {path} is missing; generate it with "
                     "tests/golden/make_ref_fixtures.py on a GPU")
     return np.load(path)
+
+
+def gauge_offset(g, case, n, ours):
+    """Uniform p offset (ours - reference) after step n from the gauges applied before it: the
+    p2 of the monitor at step k*monitor is subtracted in step k*monitor + 1."""
+    monitor = case.get("monitor", 0)
+    if not monitor:
+        return 0.0
+    ref_p2 = g[f"p2_step{max(case['steps'])}"].astype(np.float64)
+    applied = [j for j in range(len(ours)) if (j + 1) * monitor < n]
+    return float(sum(ref_p2[j] - ours[j] for j in applied))
 
 
 def rel(a, b):
@@ -59,6 +75,7 @@ def test_oracle_matches_reference_kernels(name, dtype):
                 gauge = O.monitor_ref(io, f, prm["nu"], c["lx0"] / 2, d2=RC.D)[3]
                 gauges.append(gauge)
         got = f.reshape(4, -1)[:, keep].astype(np.float64)
+        got[0] -= gauge_offset(g, c, n, gauges)
         want = g[f"step{n}"].astype(np.float64)
         ep, eu = rel(got, want)
         assert ep < TOL and eu < TOL, (name, n, ep, eu)
