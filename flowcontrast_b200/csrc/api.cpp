@@ -214,6 +214,10 @@ struct fslbm_solve {
   double* d_gauge = nullptr;
   unsigned* d_err = nullptr;
   double* d_scratch = nullptr;     // small reductions
+  // FP16 storage: stored w is the deviation from the per-column base d_wbase (lxp*ly FP32);
+  // d_wgt is the base's share of a step of the stored w (see launch_wgt)
+  float* d_wbase = nullptr;
+  float* d_wgt = nullptr;
   double* d_stats = nullptr;       // 11 * ly * (L + 2 d2) sums, then their 11 compensations
   int cnt = 0, cnt2 = 0;
   double* d_prof = nullptr;        // 10 * lxp * ly sums, then their 10 compensations
@@ -467,7 +471,7 @@ static void free_solve(fslbm_solve* s) {
   cudaSetDevice(s->ctx->device);
   void* ptrs[] = {s->state[0], s->state[1], s->d_mask, s->d_colcoef, s->d_tiles, s->d_ghosts, s->d_counters,
                   s->d_log, s->d_gauge, s->d_err, s->d_scratch, s->d_stats, s->d_prof,
-                  s->d_stage, s->d_plane};
+                  s->d_stage, s->d_plane, s->d_wbase, s->d_wgt};
   for (void* p : ptrs) ctx_free(s->ctx, p);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
@@ -658,6 +662,12 @@ extern "C" int fslbm_solve_create(fslbm_ctx* ctx, const fslbm_domain* dom, const
   if ((e = dalloc(s, &s->d_err, sizeof(unsigned)))) return fail("err");
   if ((e = cudaMemsetAsync(s->d_err, 0, sizeof(unsigned), st))) return fail("memset");
   if ((e = dalloc(s, &s->d_scratch, 8 * sizeof(double)))) return fail("scratch");
+  if (dtype == FSLBM_F16) {
+    const size_t cs = size_t(s->lxp) * s->ly * sizeof(float);
+    if ((e = dalloc(s, &s->d_wbase, cs)) || (e = dalloc(s, &s->d_wgt, cs))) return fail("w base");
+    if ((e = cudaMemsetAsync(s->d_wbase, 0, cs, st)) || (e = cudaMemsetAsync(s->d_wgt, 0, cs, st)))
+      return fail("memset");
+  }
   if (s->ghost > 0) {
     const int G = s->ghost, nx = s->lx - 2 * G, ny = s->ly - 2 * G;
     std::vector<int2> pairs;
@@ -685,6 +695,20 @@ extern "C" int fslbm_solve_destroy(fslbm_solve* s) {
   return FSLBM_OK;
 }
 
+static void fill_constants(const fslbm_solve* s, StepLaunch& a);
+
+// FP16 storage: the base's share of a step of the stored w, from the current parameters.
+static int update_wgt(fslbm_solve* s) {
+  if (!s->d_wgt) return FSLBM_OK;
+  StepLaunch a{};
+  fill_constants(s, a);
+  const float tb = float(a.tb), am = tb * float(a.dtddy) * float(a.m);
+  const float K0 = am * float(a.c0) + float(a.cc), K1 = am * float(a.c1), K2 = am * float(a.c2);
+  CUDA_TRY(launch_wgt(s->d_wbase, s->lxp, s->ly, K0, K1, K2, tb * float(a.fz), s->d_wgt,
+                      s->ctx->stream));
+  return FSLBM_OK;
+}
+
 extern "C" int fslbm_solve_set_params(fslbm_solve* s, const fslbm_params* prm) {
   if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "set_params: null solve");
   int rc = validate_params(prm, s->dtype);
@@ -695,6 +719,10 @@ extern "C" int fslbm_solve_set_params(fslbm_solve* s, const fslbm_params* prm) {
     CUDA_TRY(cudaSetDevice(s->ctx->device));
     CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
     if (int r = configure_kernel(s)) return r;
+  }
+  if (s->d_wgt) {
+    CUDA_TRY(cudaSetDevice(s->ctx->device));
+    if (int r = update_wgt(s)) return r;
   }
   return FSLBM_OK;
 }
@@ -736,13 +764,17 @@ extern "C" int fslbm_solve_set_fields(fslbm_solve* s, fslbm_dtype hd, const void
     for (int f = 0; f < 4; ++f)
       CUDA_TRY(cudaMemcpyAsync(static_cast<char*>(s->d_stage) + f * n * hes, src[f], n * hes,
                                cudaMemcpyHostToDevice, st));
+    if (s->d_wbase)                 // FP16: w is stored as the deviation from its column mean
+      CUDA_TRY(launch_wbase_dense(s->d_stage, hd == FSLBM_F64, s->d_mask, s->lx, s->lxp, s->ly, s->L,
+                                  s->d_ghosts, s->nghost, s->d_wbase, st));
     CUDA_TRY(launch_convert_in(s->dtype, dst, s->d_stage, hd == FSLBM_F64, s->lx, s->lxp, s->ly,
-                               s->L, st));
+                               s->L, st, s->d_wbase));
   }
   CUDA_TRY(launch_zero_walls(s->dtype, dst, s->d_mask, s->planes, s->lxp, s->ly, s->L, st));
   CUDA_TRY(launch_fill_ghosts(s->dtype, dst, s->d_ghosts, s->nghost, s->lxp, s->ly, s->L, st));
   // the other buffer's walls (never written by the step) must be zero too
   CUDA_TRY(launch_zero_walls(s->dtype, s->state[1 - s->cur], s->d_mask, s->planes, s->lxp, s->ly, s->L, st));
+  if (int r = update_wgt(s)) return r;
   s->fields_set = true;
   return FSLBM_OK;
 }
@@ -769,10 +801,14 @@ extern "C" int fslbm_solve_init_poiseuille(fslbm_solve* s, double umax, double n
   if (int r = fslbm_poiseuille_setup(&dom, umax, noise, modes, mode_amp, seed, &q, &fluid)) return r;
   CUDA_TRY(cudaSetDevice(s->ctx->device));
   cudaStream_t st = s->ctx->stream;
-  CUDA_TRY(launch_init_poiseuille(s->dtype, s->state[s->cur], s->d_mask, s->planes, s->lxp, q, st));
+  if (s->d_wbase)                     // FP16: w is stored as the deviation from the profile
+    CUDA_TRY(launch_wbase_poiseuille(s->d_mask, s->lxp, q, s->d_ghosts, s->nghost, s->d_wbase, st));
+  CUDA_TRY(launch_init_poiseuille(s->dtype, s->state[s->cur], s->d_mask, s->planes, s->lxp, q, st,
+                                  s->d_wbase));
   CUDA_TRY(launch_fill_ghosts(s->dtype, s->state[s->cur], s->d_ghosts, s->nghost, s->lxp, s->ly,
                               s->L, st));
   CUDA_TRY(launch_zero_walls(s->dtype, s->state[1 - s->cur], s->d_mask, s->planes, s->lxp, s->ly, s->L, st));
+  if (int r = update_wgt(s)) return r;
   s->fields_set = true;
   return FSLBM_OK;
 }
@@ -792,7 +828,8 @@ extern "C" int fslbm_solve_footprint(const fslbm_domain* dom, fslbm_dtype dtype,
                             ? cs * dom->lz * (1 + int64_t(dtype == FSLBM_F64 ? sizeof(CellCoef<double>)
                                                                                 : sizeof(CellCoef<float>)))
                             : cs + cs * cc;
-  *bytes = 2 * 4 * fs * es + masks + tiles + int64_t(sizeof(DevCounters)) +
+  const int64_t wtabs = dtype == FSLBM_F16 ? 2 * cs * int64_t(sizeof(float)) : 0;
+  *bytes = 2 * 4 * fs * es + masks + tiles + wtabs + int64_t(sizeof(DevCounters)) +
            4096 * int64_t(sizeof(fslbm_monitor)) + int64_t(sizeof(double)) * 9 + int64_t(sizeof(unsigned));
   return FSLBM_OK;
 }
@@ -816,7 +853,7 @@ extern "C" int fslbm_solve_get_fields(fslbm_solve* s, fslbm_dtype hd, void* p, v
   } else {
     if (int r = ensure_stage(s, 4 * n * hes)) return r;
     CUDA_TRY(launch_convert_out(s->dtype, src, s->d_stage, hd == FSLBM_F64, s->lx, s->lxp, s->ly,
-                                s->L, st));
+                                s->L, st, s->d_wbase));
     for (int f = 0; f < 4; ++f)
       CUDA_TRY(cudaMemcpyAsync(dst[f], static_cast<char*>(s->d_stage) + f * n * hes, n * hes,
                                cudaMemcpyDeviceToHost, st));
@@ -861,6 +898,7 @@ static int enqueue_steps(fslbm_solve* s, int64_t nsteps) {
   a.ntiles = s->ntiles; a.chunk = s->chunk; a.nchunks = s->nchunks;
   a.tiles = s->d_tiles; a.mask = s->d_mask; a.colcoef = s->d_colcoef;
   a.err = s->d_err; a.counters = s->d_counters; a.mask_planes = s->planes;
+  a.wb = s->d_wbase; a.wgt = s->d_wgt;
   fill_constants(s, a);
   MonitorLaunch m{};
   m.dtype = s->dtype; m.mask = s->d_mask;
@@ -869,6 +907,7 @@ static int enqueue_steps(fslbm_solve* s, int64_t nsteps) {
   m.nu = s->prm.nu; m.radius = s->radius; m.l1 = s->l1;
   m.sx = s->sx; m.sy = s->sy; m.sz = s->sz;
   m.log = s->d_log; m.log_cap = s->log_cap; m.gauge_out = s->d_gauge; m.counters = s->d_counters;
+  m.wb = s->d_wbase;
   const int me = s->prm.monitor_every;
   for (int64_t n = 0; n < nsteps; ++n) {
     const int64_t c = s->steps + 1;
@@ -966,7 +1005,8 @@ extern "C" int fslbm_solve_monitor(fslbm_solve* s, fslbm_monitor* out) {
 extern "C" int fslbm_solve_check(fslbm_solve* s, double* max_abs_u) {
   if (!s) return fslbm_set_error(FSLBM_ERR_ARG, "check: null solve");
   CUDA_TRY(cudaSetDevice(s->ctx->device));
-  CUDA_TRY(launch_check(s->dtype, s->state[s->cur], field_stride(s), s->d_scratch, s->ctx->stream));
+  CUDA_TRY(launch_check(s->dtype, s->state[s->cur], field_stride(s), s->d_scratch, s->ctx->stream,
+                        s->lxp, s->ly, s->d_wbase));
   double r[2];
   CUDA_TRY(cudaMemcpyAsync(r, s->d_scratch, sizeof r, cudaMemcpyDeviceToHost, s->ctx->stream));
   CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
@@ -1072,7 +1112,7 @@ extern "C" int fslbm_solve_get_plane(fslbm_solve* s, int kind, int comp, float* 
   if (kind == 0) {
     const int xs = s->lx / 2;
     CUDA_TRY(launch_gather_plane(s->dtype, s->state[s->cur], s->lx, s->lxp, s->ly, s->L, 0, xs,
-                                 s->d_plane, st));
+                                 s->d_plane, st, s->d_wbase));
     buf.resize(4 * size_t(s->L) * s->ly);
     CUDA_TRY(cudaMemcpyAsync(buf.data(), s->d_plane, buf.size() * sizeof(float),
                              cudaMemcpyDeviceToHost, st));
@@ -1093,7 +1133,7 @@ extern "C" int fslbm_solve_get_plane(fslbm_solve* s, int kind, int comp, float* 
     int zr = Lr / 2, zc = zr - s->d2, jump = 0;
     if (zc < 0) { zc += s->L; jump = 1; } else if (zc >= s->L) { zc -= s->L; jump = -1; }
     CUDA_TRY(launch_gather_plane(s->dtype, s->state[s->cur], s->lx, s->lxp, s->ly, s->L, 1, zc,
-                                 s->d_plane, st));
+                                 s->d_plane, st, s->d_wbase));
     const size_t n = size_t(s->ly) * s->lx;
     buf.resize(4 * n);
     CUDA_TRY(cudaMemcpyAsync(buf.data(), s->d_plane, buf.size() * sizeof(float),
@@ -1141,7 +1181,7 @@ extern "C" int fslbm_stats_sample(fslbm_solve* s) {
   s->cnt += 1; s->cnt2 += 1;                                   // FSLBM.cu:715
   const double pin = s->dtype != FSLBM_F64 ? double(float(s->prm.pin)) : s->prm.pin;
   CUDA_TRY(launch_plane_stats(s->dtype, s->state[s->cur], s->d_mask, s->planes, s->lxp, s->ly, s->L, s->d2,
-                              s->lx / 2, pin, s->cnt, 1, 1, s->d_stats, st));
+                              s->lx / 2, pin, s->cnt, 1, 1, s->d_stats, st, s->d_wbase));
   return FSLBM_OK;
 }
 
@@ -1186,7 +1226,8 @@ extern "C" int fslbm_profile_sample(fslbm_solve* s) {
     CUDA_TRY(dalloc(s, &s->d_prof, 20 * n * sizeof(double)));
     CUDA_TRY(cudaMemsetAsync(s->d_prof, 0, 20 * n * sizeof(double), s->ctx->stream));
   }
-  CUDA_TRY(launch_profile(s->dtype, s->state[s->cur], s->lxp, s->ly, s->L, s->d_prof, s->ctx->stream));
+  CUDA_TRY(launch_profile(s->dtype, s->state[s->cur], s->lxp, s->ly, s->L, s->d_prof, s->ctx->stream,
+                          s->d_wbase));
   s->prof_n += 1;
   return FSLBM_OK;
 }
@@ -1326,6 +1367,7 @@ static int batch_upload(fslbm_batch* b) {
     a.lxp = s->lxp; a.ly = s->ly; a.L = s->L; a.ntiles = s->ntiles;
     a.tiles = s->d_tiles; a.mask = s->d_mask; a.colcoef = s->d_colcoef;
     a.err = b->d_tickets + 2;        // one flag for the whole batch
+    a.wb = s->d_wbase; a.wgt = s->d_wgt;
     fill_constants(s, a);
     const int nch = member_chunks(s, eff_chunk(i));
     const long long stop_at = b->stop[i] >= 0 ? (long long)b->stop[i] : LLONG_MAX;
@@ -1356,6 +1398,7 @@ static int batch_upload(fslbm_batch* b) {
     m.mon.l1 = s->l1; m.mon.sx = s->sx; m.mon.sy = s->sy; m.mon.sz = s->sz;
     m.mon.log = s->d_log; m.mon.log_cap = s->log_cap; m.mon.gauge_out = s->d_gauge;
     m.mon.counters = s->d_counters;
+    m.mon.wb = s->d_wbase;
     m.state[0] = s->state[0]; m.state[1] = s->state[1];
     m.stop_at = stop_at;
     m.monitor_every = s->prm.monitor_every; m.cur0 = s->cur;

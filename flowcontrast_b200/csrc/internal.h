@@ -46,6 +46,8 @@ struct StepLaunch {
   long long step_no;         // the time step this launch computes (1-based; rounding seed)
   int K;                     // corrector taps (2: the reference's order 2<->4 blend)
   int mask_planes;           // 0/1: extruded cross-section; L: a mask (and CellCoef) per plane
+  const float* wb;           // FP16 storage: per-column base of w and its step share, else null
+  const float* wgt;
   // constants in double; converted to the compute type by the launcher
   double tb, cc, pin, dtddy, m, c0, c1, c2, fx, fy, fz;
   double ch[6];              // corrector coefficients c3..c8
@@ -87,6 +89,7 @@ struct MonitorLaunch {
   int log_cap;
   double* gauge_out;
   DevCounters* counters;
+  const float* wb = nullptr;  // FP16 storage: per-column base of w (stored w is w - wb)
 };
 cudaError_t launch_monitor(const MonitorLaunch& a, cudaStream_t st);
 // The bounded waits against conditions nothing satisfies (counter stays 0): err bit 0 = the
@@ -121,7 +124,8 @@ cudaError_t launch_batch_steps(int dtype, const void* members, const BatchMon* m
 
 // Seeded Poiseuille start written into a pitched state (walls and pad columns zero).
 cudaError_t launch_init_poiseuille(int dtype, void* state, const uint8_t* mask, int planes, int lxp,
-                                   const PoiseuilleInit& q, cudaStream_t st);
+                                   const PoiseuilleInit& q, cudaStream_t st,
+                                   const float* wb = nullptr);
 // Periodic cross-section: pairs (ghost cell, interior image) as cross-section indices.
 cudaError_t launch_fill_ghosts(int dtype, void* state, const int2* pairs, int n, int lxp, int ly,
                                int L, cudaStream_t st);
@@ -130,17 +134,29 @@ cudaError_t launch_zero_walls(int dtype, void* state, const uint8_t* mask, int p
                               int ly, int L, cudaStream_t st);
 cudaError_t launch_plane_stats(int dtype, const void* state, const uint8_t* mask, int planes, int lxp, int ly,
                                int L, int d2, int xs, double pin, int cnt, int do_mean,
-                               int do_fluct, double* acc, cudaStream_t st);
+                               int do_fluct, double* acc, cudaStream_t st, const float* wb = nullptr);
 cudaError_t launch_profile(int dtype, const void* state, int lxp, int ly, int L, double* acc,
-                           cudaStream_t st);
+                           cudaStream_t st, const float* wb = nullptr);
 cudaError_t launch_check(int dtype, const void* state, size_t n_per_field, double* out,
-                         cudaStream_t st);
+                         cudaStream_t st, int lxp = 0, int ly = 0, const float* wb = nullptr);
 // Converts between the storage type and FP32/FP64 staging buffers (dense per field, pitched).
 // src/dst: dense [4][L][ly][lx] staging arrays; state: pitched [4][L][ly][lxp].
 cudaError_t launch_convert_in(int dtype, void* state, const void* src, int src_is_f64, int lx,
-                              int lxp, int ly, int L, cudaStream_t st);
+                              int lxp, int ly, int L, cudaStream_t st, const float* wb = nullptr);
 cudaError_t launch_convert_out(int dtype, const void* state, void* dst, int dst_is_f64, int lx,
-                               int lxp, int ly, int L, cudaStream_t st);
+                               int lxp, int ly, int L, cudaStream_t st, const float* wb = nullptr);
+// FP16 storage keeps w as a deviation from a per-column FP32 base wb (lxp*ly): the streamwise
+// mean of the given fields' w (set_fields) or the analytic Poiseuille profile (init_poiseuille),
+// zero on wall and padding columns; ghost columns of a periodic cross-section take their
+// images' base. wgt holds the base's share of the step of the stored w (corrector taps of the
+// base and the body force, per column), recomputed when the parameters change.
+cudaError_t launch_wbase_dense(const void* src, int src_is_f64, const uint8_t* mask, int lx, int lxp,
+                               int ly, int L, const int2* ghosts, int nghost, float* wb,
+                               cudaStream_t st);
+cudaError_t launch_wbase_poiseuille(const uint8_t* mask, int lxp, const PoiseuilleInit& q,
+                                    const int2* ghosts, int nghost, float* wb, cudaStream_t st);
+cudaError_t launch_wgt(const float* wb, int lxp, int ly, float K0, float K1, float K2, float tfz,
+                       float* wgt, cudaStream_t st);
 
 }  // namespace fslbm
 
@@ -154,5 +170,6 @@ int fd_coefficients(int order, double blend, int fp32, double* c);
 // Gathers the YZ plane x = idx (kind 0, out [4][L][ly]) or the XY plane z = idx
 // (kind 1, out [4][ly][lx]) of the four fields as FP32 into device memory.
 cudaError_t launch_gather_plane(int dtype, const void* state, int lx, int lxp, int ly, int L,
-                                int kind, int idx, float* out, cudaStream_t st);
+                                int kind, int idx, float* out, cudaStream_t st,
+                                const float* wb = nullptr);
 }  // namespace fslbm

@@ -16,6 +16,14 @@ template <> struct ArithOf<__half> { using type = float; };
 __device__ __forceinline__ double to_d(float x) { return double(x); }
 __device__ __forceinline__ double to_d(double x) { return x; }
 __device__ __forceinline__ double to_d(__half x) { return double(__half2float(x)); }
+// A stored value as its field's value: FP16 storage keeps w as a deviation from the per-column
+// base wb (w = stored + base in FP32, as the step forms it); other types and fields are as stored.
+template <class TS> __device__ __forceinline__ double wval(TS v, const float*, size_t) {
+  return to_d(v);
+}
+template <> __device__ __forceinline__ double wval<__half>(__half v, const float* wb, size_t col) {
+  return wb ? double(__fadd_rn(__half2float(v), wb[col])) : to_d(v);
+}
 
 // ------------------------------------------------------------------------------------------
 // step dispatch
@@ -194,6 +202,8 @@ cudaError_t launch_step2(const StepLaunch& a, const Step2Launch& b, cudaStream_t
   g.lxp = a.lxp; g.ly = a.ly; g.L = a.L; g.ntiles = a.ntiles; g.nchunks = b.grid / a.ntiles;
   g.tiles = a.tiles; g.mask = a.mask; g.colcoef = a.colcoef; g.out = a.out;
   g.gauge = a.gauge; g.err = a.err;
+  g.wb = a.wb; g.wgt = a.wgt;
+  g.wb = a.wb; g.wgt = a.wgt;
   g.step_counter = a.counters ? &a.counters->steps : nullptr;
   g.step_no = unsigned(a.step_no);
   StepConst<float> k;
@@ -255,7 +265,7 @@ __device__ void monitor_body(const MonitorLaunch& a, double* sh) {
   for (int j = threadIdx.x; j < a.lxp * a.ly; j += blockDim.x) {
     if (a.mask[j] != 0) continue;           // walls hold zero; periodic images are not counted
     const TA p = TA(__ldcg(st + j));
-    v[0] += to_d(__ldcg(st + 3 * FS + j));
+    v[0] += wval(__ldcg(st + 3 * FS + j), a.wb, size_t(j));
     v[1] += double(p);
     v[2] += double(TA(p - pin));            // the outlet buffer copy's p
   }
@@ -266,7 +276,8 @@ __device__ void monitor_body(const MonitorLaunch& a, double* sh) {
     r.step = a.counters->steps;
     r.q1 = q1; r.q2 = q1; r.p1 = p1; r.p2 = p2;
     r.f = (p1 - p2) / q1 / q1 / 3.0 * 4.0 * a.radius / double(a.L);
-    r.sample = to_d(__ldcg(st + 3 * FS + (size_t(a.sz) * a.ly + a.sy) * a.lxp + a.sx));
+    r.sample = wval(__ldcg(st + 3 * FS + (size_t(a.sz) * a.ly + a.sy) * a.lxp + a.sx), a.wb,
+                    size_t(a.sy) * a.lxp + a.sx);
     r.re = 2.0 * a.radius * q1 / a.nu;
     const long long idx = a.counters->records;
     a.log[idx % a.log_cap] = r;
@@ -453,6 +464,7 @@ cudaError_t fill_batch_member(void* dst, const CUtensorMap* mp, const CUtensorMa
   m.g.lxp = a.lxp; m.g.ly = a.ly; m.g.L = a.L; m.g.ntiles = a.ntiles; m.g.nchunks = nchunks;
   m.g.tiles = a.tiles; m.g.mask = a.mask; m.g.colcoef = a.colcoef; m.g.out = nullptr;
   m.g.gauge = nullptr; m.g.err = a.err; m.g.step_counter = nullptr; m.g.step_no = 0;
+  m.g.wb = a.wb; m.g.wgt = a.wgt;
   StepConst<float> k;
   k.tb = float(a.tb); k.cc = float(a.cc); k.pin = float(a.pin); k.dtddy = float(a.dtddy);
   k.m = float(a.m); k.c0 = float(a.c0); k.c1 = float(a.c1); k.c2 = float(a.c2);
@@ -503,7 +515,7 @@ cudaError_t launch_monitor(const MonitorLaunch& a, cudaStream_t st) {
 // ------------------------------------------------------------------------------------------
 template <class TS>
 __global__ void init_poiseuille_kernel(TS* s, const uint8_t* mask, int planes, int lxp,
-                                       PoiseuilleInit q) {
+                                       PoiseuilleInit q, const float* wb) {
   const size_t FS = size_t(lxp) * q.ly * q.L;
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < FS;
        i += size_t(gridDim.x) * blockDim.x) {
@@ -513,19 +525,21 @@ __global__ void init_poiseuille_kernel(TS* s, const uint8_t* mask, int planes, i
     double c[4] = {0.0, 0.0, 0.0, 0.0};
     if (x < q.lx && mask[(planes > 1 ? size_t(z) * q.ly : 0) * lxp + size_t(y) * lxp + x] != kWall)
       poiseuille_cell(q, x, y, z, c);
-    s[i] = TS(c[0]); s[FS + i] = TS(c[1]); s[2 * FS + i] = TS(c[2]); s[3 * FS + i] = TS(c[3]);
+    s[i] = TS(c[0]); s[FS + i] = TS(c[1]); s[2 * FS + i] = TS(c[2]);
+    if (wb) s[3 * FS + i] = TS(__fsub_rn(float(c[3]), wb[size_t(y) * lxp + x]));
+    else s[3 * FS + i] = TS(c[3]);
   }
 }
 
 cudaError_t launch_init_poiseuille(int dtype, void* state, const uint8_t* mask, int planes, int lxp,
-                                   const PoiseuilleInit& q, cudaStream_t st) {
+                                   const PoiseuilleInit& q, cudaStream_t st, const float* wb) {
   const int grid = 1184;
   if (dtype == FSLBM_F32)
-    init_poiseuille_kernel<float><<<grid, 256, 0, st>>>((float*)state, mask, planes, lxp, q);
+    init_poiseuille_kernel<float><<<grid, 256, 0, st>>>((float*)state, mask, planes, lxp, q, nullptr);
   else if (dtype == FSLBM_F64)
-    init_poiseuille_kernel<double><<<grid, 256, 0, st>>>((double*)state, mask, planes, lxp, q);
+    init_poiseuille_kernel<double><<<grid, 256, 0, st>>>((double*)state, mask, planes, lxp, q, nullptr);
   else if (dtype == FSLBM_F16)
-    init_poiseuille_kernel<__half><<<grid, 256, 0, st>>>((__half*)state, mask, planes, lxp, q);
+    init_poiseuille_kernel<__half><<<grid, 256, 0, st>>>((__half*)state, mask, planes, lxp, q, wb);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -590,7 +604,8 @@ cudaError_t launch_zero_walls(int dtype, void* state, const uint8_t* mask, int p
 // Dense host-layout fields (4 x L x ly x lx) <-> the pitched state (4 x L x ly x lxp), with a type
 // conversion. A warp copies one row at a time (one division per row, coalesced along x).
 template <class TS, class TH>
-__global__ void convert_in_kernel(TS* s, const TH* src, int lx, int lxp, int ly, int L) {
+__global__ void convert_in_kernel(TS* s, const TH* src, int lx, int lxp, int ly, int L,
+                                  const float* wb) {
   const long long rows = (long long)ly * L, FS = (long long)lxp * rows;
   const int lane = threadIdx.x & 31;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -599,11 +614,17 @@ __global__ void convert_in_kernel(TS* s, const TH* src, int lx, int lxp, int ly,
     const long long f = rr / rows, yz = rr - f * rows;
     const TH* in = src + rr * lx;
     TS* out = s + f * FS + yz * lxp;
-    for (int x = lane; x < lx; x += 32) out[x] = TS(in[x]);
+    if (wb && f == 3) {                 // FP16 storage: w as the deviation from its base
+      const float* b = wb + (yz % ly) * lxp;
+      for (int x = lane; x < lx; x += 32) out[x] = TS(__fsub_rn(float(in[x]), b[x]));
+    } else {
+      for (int x = lane; x < lx; x += 32) out[x] = TS(in[x]);
+    }
   }
 }
 template <class TS, class TH>
-__global__ void convert_out_kernel(const TS* s, TH* dst, int lx, int lxp, int ly, int L) {
+__global__ void convert_out_kernel(const TS* s, TH* dst, int lx, int lxp, int ly, int L,
+                                   const float* wb) {
   const long long rows = (long long)ly * L, FS = (long long)lxp * rows;
   const int lane = threadIdx.x & 31;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -612,50 +633,55 @@ __global__ void convert_out_kernel(const TS* s, TH* dst, int lx, int lxp, int ly
     const long long f = rr / rows, yz = rr - f * rows;
     const TS* in = s + f * FS + yz * lxp;
     TH* out = dst + rr * lx;
-    for (int x = lane; x < lx; x += 32) out[x] = TH(in[x]);
+    if (wb && f == 3) {
+      const size_t row = size_t(yz % ly) * lxp;
+      for (int x = lane; x < lx; x += 32) out[x] = TH(wval(in[x], wb, row + x));
+    } else {
+      for (int x = lane; x < lx; x += 32) out[x] = TH(in[x]);
+    }
   }
 }
 
 cudaError_t launch_convert_in(int dtype, void* state, const void* src, int src_is_f64, int lx,
-                              int lxp, int ly, int L, cudaStream_t st) {
+                              int lxp, int ly, int L, cudaStream_t st, const float* wb) {
   const int grid = 1184;
   if (dtype == FSLBM_F32) {
-    if (src_is_f64) convert_in_kernel<float, double><<<grid, 256, 0, st>>>((float*)state, (const double*)src, lx, lxp, ly, L);
-    else convert_in_kernel<float, float><<<grid, 256, 0, st>>>((float*)state, (const float*)src, lx, lxp, ly, L);
+    if (src_is_f64) convert_in_kernel<float, double><<<grid, 256, 0, st>>>((float*)state, (const double*)src, lx, lxp, ly, L, nullptr);
+    else convert_in_kernel<float, float><<<grid, 256, 0, st>>>((float*)state, (const float*)src, lx, lxp, ly, L, nullptr);
   } else if (dtype == FSLBM_F64) {
-    if (src_is_f64) convert_in_kernel<double, double><<<grid, 256, 0, st>>>((double*)state, (const double*)src, lx, lxp, ly, L);
-    else convert_in_kernel<double, float><<<grid, 256, 0, st>>>((double*)state, (const float*)src, lx, lxp, ly, L);
+    if (src_is_f64) convert_in_kernel<double, double><<<grid, 256, 0, st>>>((double*)state, (const double*)src, lx, lxp, ly, L, nullptr);
+    else convert_in_kernel<double, float><<<grid, 256, 0, st>>>((double*)state, (const float*)src, lx, lxp, ly, L, nullptr);
   } else if (dtype == FSLBM_F16) {
-    if (src_is_f64) convert_in_kernel<__half, double><<<grid, 256, 0, st>>>((__half*)state, (const double*)src, lx, lxp, ly, L);
-    else convert_in_kernel<__half, float><<<grid, 256, 0, st>>>((__half*)state, (const float*)src, lx, lxp, ly, L);
+    if (src_is_f64) convert_in_kernel<__half, double><<<grid, 256, 0, st>>>((__half*)state, (const double*)src, lx, lxp, ly, L, wb);
+    else convert_in_kernel<__half, float><<<grid, 256, 0, st>>>((__half*)state, (const float*)src, lx, lxp, ly, L, wb);
   } else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 
 cudaError_t launch_convert_out(int dtype, const void* state, void* dst, int dst_is_f64, int lx,
-                               int lxp, int ly, int L, cudaStream_t st) {
+                               int lxp, int ly, int L, cudaStream_t st, const float* wb) {
   const int grid = 1184;
   if (dtype == FSLBM_F32) {
-    if (dst_is_f64) convert_out_kernel<float, double><<<grid, 256, 0, st>>>((const float*)state, (double*)dst, lx, lxp, ly, L);
-    else convert_out_kernel<float, float><<<grid, 256, 0, st>>>((const float*)state, (float*)dst, lx, lxp, ly, L);
+    if (dst_is_f64) convert_out_kernel<float, double><<<grid, 256, 0, st>>>((const float*)state, (double*)dst, lx, lxp, ly, L, nullptr);
+    else convert_out_kernel<float, float><<<grid, 256, 0, st>>>((const float*)state, (float*)dst, lx, lxp, ly, L, nullptr);
   } else if (dtype == FSLBM_F64) {
-    if (dst_is_f64) convert_out_kernel<double, double><<<grid, 256, 0, st>>>((const double*)state, (double*)dst, lx, lxp, ly, L);
-    else convert_out_kernel<double, float><<<grid, 256, 0, st>>>((const double*)state, (float*)dst, lx, lxp, ly, L);
+    if (dst_is_f64) convert_out_kernel<double, double><<<grid, 256, 0, st>>>((const double*)state, (double*)dst, lx, lxp, ly, L, nullptr);
+    else convert_out_kernel<double, float><<<grid, 256, 0, st>>>((const double*)state, (float*)dst, lx, lxp, ly, L, nullptr);
   } else if (dtype == FSLBM_F16) {
-    if (dst_is_f64) convert_out_kernel<__half, double><<<grid, 256, 0, st>>>((const __half*)state, (double*)dst, lx, lxp, ly, L);
-    else convert_out_kernel<__half, float><<<grid, 256, 0, st>>>((const __half*)state, (float*)dst, lx, lxp, ly, L);
+    if (dst_is_f64) convert_out_kernel<__half, double><<<grid, 256, 0, st>>>((const __half*)state, (double*)dst, lx, lxp, ly, L, wb);
+    else convert_out_kernel<__half, float><<<grid, 256, 0, st>>>((const __half*)state, (float*)dst, lx, lxp, ly, L, wb);
   } else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 
 // out[0] = number of non-finite values, out[1] = max |u|,|v|,|w| (FP64)
 template <class TS>
-__global__ void check_kernel(const TS* s, size_t n, double* out) {
+__global__ void check_kernel(const TS* s, size_t n, double* out, size_t plane, const float* wb) {
   __shared__ double sh[2 * 32];
   double v[2] = {0, 0};
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < 4 * n;
        i += size_t(gridDim.x) * blockDim.x) {
-    const double a = to_d(s[i]);
+    const double a = (wb && i >= 3 * n) ? wval(s[i], wb, (i - 3 * n) % plane) : to_d(s[i]);
     if (!isfinite(a)) v[0] += 1.0;
     else if (i >= n) v[1] = fmax(v[1], fabs(a));
   }
@@ -683,12 +709,13 @@ __global__ void check_kernel(const TS* s, size_t n, double* out) {
 }
 
 cudaError_t launch_check(int dtype, const void* state, size_t n_per_field, double* out,
-                         cudaStream_t st) {
+                         cudaStream_t st, int lxp, int ly, const float* wb) {
   cudaError_t e = cudaMemsetAsync(out, 0, 2 * sizeof(double), st);
   if (e) return e;
-  if (dtype == FSLBM_F32) check_kernel<float><<<296, 256, 0, st>>>((const float*)state, n_per_field, out);
-  else if (dtype == FSLBM_F64) check_kernel<double><<<296, 256, 0, st>>>((const double*)state, n_per_field, out);
-  else if (dtype == FSLBM_F16) check_kernel<__half><<<296, 256, 0, st>>>((const __half*)state, n_per_field, out);
+  const size_t plane = size_t(lxp) * ly;
+  if (dtype == FSLBM_F32) check_kernel<float><<<296, 256, 0, st>>>((const float*)state, n_per_field, out, plane, nullptr);
+  else if (dtype == FSLBM_F64) check_kernel<double><<<296, 256, 0, st>>>((const double*)state, n_per_field, out, plane, nullptr);
+  else if (dtype == FSLBM_F16) check_kernel<__half><<<296, 256, 0, st>>>((const __half*)state, n_per_field, out, plane, plane ? wb : nullptr);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -714,7 +741,8 @@ __device__ __forceinline__ void comp_add(double* s, double* c, double x) {
 // ------------------------------------------------------------------------------------------
 template <class TS>
 __global__ void plane_stats_kernel(const TS* s, const uint8_t* mask, int planes, int lxp, int ly,
-                                   int L, int d2, int xs, double pin_d, int cnt, double* acc) {
+                                   int L, int d2, int xs, double pin_d, int cnt, double* acc,
+                                   const float* wb) {
   const int Lr = L + 2 * d2;
   const size_t n = size_t(ly) * Lr, FS = size_t(lxp) * ly * L;
   using TA = typename ArithOf<TS>::type;
@@ -731,7 +759,8 @@ __global__ void plane_stats_kernel(const TS* s, const uint8_t* mask, int planes,
       if (jump == 1) p = TA(p + pin);
       else if (jump == -1) p = TA(p - pin);
     }
-    const double q[4] = {double(p), to_d(s[FS + o]), to_d(s[2 * FS + o]), to_d(s[3 * FS + o])};
+    const double q[4] = {double(p), to_d(s[FS + o]), to_d(s[2 * FS + o]),
+                         wval(s[3 * FS + o], wb, size_t(y) * lxp + xs)};
     const double c = double(cnt);
     double dd[4];
 #pragma unroll
@@ -749,14 +778,14 @@ __global__ void plane_stats_kernel(const TS* s, const uint8_t* mask, int planes,
 
 cudaError_t launch_plane_stats(int dtype, const void* state, const uint8_t* mask, int planes, int lxp, int ly,
                                int L, int d2, int xs, double pin, int cnt, int, int, double* acc,
-                               cudaStream_t st) {
+                               cudaStream_t st, const float* wb) {
   const int grid = 148;
   if (dtype == FSLBM_F32)
-    plane_stats_kernel<float><<<grid, 256, 0, st>>>((const float*)state, mask, planes, lxp, ly, L, d2, xs, pin, cnt, acc);
+    plane_stats_kernel<float><<<grid, 256, 0, st>>>((const float*)state, mask, planes, lxp, ly, L, d2, xs, pin, cnt, acc, nullptr);
   else if (dtype == FSLBM_F64)
-    plane_stats_kernel<double><<<grid, 256, 0, st>>>((const double*)state, mask, planes, lxp, ly, L, d2, xs, pin, cnt, acc);
+    plane_stats_kernel<double><<<grid, 256, 0, st>>>((const double*)state, mask, planes, lxp, ly, L, d2, xs, pin, cnt, acc, nullptr);
   else if (dtype == FSLBM_F16)
-    plane_stats_kernel<__half><<<grid, 256, 0, st>>>((const __half*)state, mask, planes, lxp, ly, L, d2, xs, pin, cnt, acc);
+    plane_stats_kernel<__half><<<grid, 256, 0, st>>>((const __half*)state, mask, planes, lxp, ly, L, d2, xs, pin, cnt, acc, wb);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -769,7 +798,7 @@ cudaError_t launch_plane_stats(int dtype, const void* state, const uint8_t* mask
 // then 10 arrays of their compensations.
 // ------------------------------------------------------------------------------------------
 template <class TS>
-__global__ void profile_kernel(const TS* s, int lxp, int ly, int L, double* acc) {
+__global__ void profile_kernel(const TS* s, int lxp, int ly, int L, double* acc, const float* wb) {
   __shared__ double sh[10][8][33];
   const int tx = threadIdx.x & 31, tz = threadIdx.x >> 5;
   const int x = blockIdx.x * 32 + tx, y = blockIdx.y;
@@ -779,7 +808,7 @@ __global__ void profile_kernel(const TS* s, int lxp, int ly, int L, double* acc)
     for (int z = tz; z < L; z += 8) {
       const size_t o = (size_t(z) * ly + y) * lxp + x;
       const double p = to_d(s[o]), u = to_d(s[FS + o]), vv = to_d(s[2 * FS + o]),
-                   w = to_d(s[3 * FS + o]);
+                   w = wval(s[3 * FS + o], wb, size_t(y) * lxp + x);
       v[0] += p; v[1] += u; v[2] += vv; v[3] += w;
       v[4] += u * u; v[5] += vv * vv; v[6] += w * w; v[7] += u * vv; v[8] += u * w; v[9] += vv * w;
     }
@@ -799,11 +828,11 @@ __global__ void profile_kernel(const TS* s, int lxp, int ly, int L, double* acc)
 }
 
 cudaError_t launch_profile(int dtype, const void* state, int lxp, int ly, int L, double* acc,
-                           cudaStream_t st) {
+                           cudaStream_t st, const float* wb) {
   dim3 grid((lxp + 31) / 32, ly, 1);
-  if (dtype == FSLBM_F32) profile_kernel<float><<<grid, 256, 0, st>>>((const float*)state, lxp, ly, L, acc);
-  else if (dtype == FSLBM_F64) profile_kernel<double><<<grid, 256, 0, st>>>((const double*)state, lxp, ly, L, acc);
-  else if (dtype == FSLBM_F16) profile_kernel<__half><<<grid, 256, 0, st>>>((const __half*)state, lxp, ly, L, acc);
+  if (dtype == FSLBM_F32) profile_kernel<float><<<grid, 256, 0, st>>>((const float*)state, lxp, ly, L, acc, nullptr);
+  else if (dtype == FSLBM_F64) profile_kernel<double><<<grid, 256, 0, st>>>((const double*)state, lxp, ly, L, acc, nullptr);
+  else if (dtype == FSLBM_F16) profile_kernel<__half><<<grid, 256, 0, st>>>((const __half*)state, lxp, ly, L, acc, wb);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -826,7 +855,7 @@ bool step_box(int dtype, int d1, int K, int* sw, int* sh, int* hx, int* hy) {
 
 template <class TS>
 __global__ void gather_plane_kernel(const TS* s, int lx, int lxp, int ly, int L, int kind, int idx,
-                                    float* out) {
+                                    float* out, const float* wb) {
   const size_t FS = size_t(lxp) * ly * L;
   const size_t n = kind == 0 ? size_t(L) * ly : size_t(ly) * lx;
   for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < 4 * n;
@@ -835,18 +864,18 @@ __global__ void gather_plane_kernel(const TS* s, int lx, int lxp, int ly, int L,
     size_t o;
     if (kind == 0) o = (r / ly * ly + r % ly) * lxp + idx;          // r = y + ly*z
     else o = (size_t(idx) * ly + r / lx) * lxp + r % lx;            // r = x + lx*y
-    out[k] = float(to_d(s[f * FS + o]));
+    out[k] = float(f == 3 ? wval(s[f * FS + o], wb, o % (size_t(lxp) * ly)) : to_d(s[f * FS + o]));
   }
 }
 
 cudaError_t launch_gather_plane(int dtype, const void* state, int lx, int lxp, int ly, int L,
-                                int kind, int idx, float* out, cudaStream_t st) {
+                                int kind, int idx, float* out, cudaStream_t st, const float* wb) {
   if (dtype == FSLBM_F32)
-    gather_plane_kernel<float><<<148, 256, 0, st>>>((const float*)state, lx, lxp, ly, L, kind, idx, out);
+    gather_plane_kernel<float><<<148, 256, 0, st>>>((const float*)state, lx, lxp, ly, L, kind, idx, out, nullptr);
   else if (dtype == FSLBM_F64)
-    gather_plane_kernel<double><<<148, 256, 0, st>>>((const double*)state, lx, lxp, ly, L, kind, idx, out);
+    gather_plane_kernel<double><<<148, 256, 0, st>>>((const double*)state, lx, lxp, ly, L, kind, idx, out, nullptr);
   else if (dtype == FSLBM_F16)
-    gather_plane_kernel<__half><<<148, 256, 0, st>>>((const __half*)state, lx, lxp, ly, L, kind, idx, out);
+    gather_plane_kernel<__half><<<148, 256, 0, st>>>((const __half*)state, lx, lxp, ly, L, kind, idx, out, wb);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -872,6 +901,88 @@ __global__ void wait_selftest_kernel(const unsigned* counter, unsigned long long
 cudaError_t launch_wait_selftest(const unsigned* counter, unsigned long long limit_ns, unsigned* err,
                                  cudaStream_t st) {
   wait_selftest_kernel<<<1, 32, 0, st>>>(counter, limit_ns, err);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------
+// FP16 storage: the per-column base of w and its share of the step
+// ------------------------------------------------------------------------------------------
+// Base from dense host-layout fields (4 x L x ly x lx): the streamwise mean of w per non-wall
+// column x < lx (FP64 sum in z order), zero elsewhere.
+template <class TH>
+__global__ void wbase_dense_kernel(const TH* src, const uint8_t* mask, int lx, int lxp, int ly,
+                                   int L, float* wb) {
+  const size_t n = size_t(lx) * ly * L;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < lxp * ly; i += gridDim.x * blockDim.x) {
+    const int x = i % lxp, y = i / lxp;
+    float b = 0.0f;
+    if (x < lx && mask[i] != kWall) {
+      double sum = 0.0;
+      for (int z = 0; z < L; ++z) sum += double(src[3 * n + (size_t(z) * ly + y) * lx + x]);
+      b = float(sum / double(L));
+    }
+    wb[i] = b;
+  }
+}
+// The analytic Poiseuille profile of a seeded start: -umax (1 - r^2/R^2) on non-wall columns.
+__global__ void wbase_poiseuille_kernel(const uint8_t* mask, int lxp, PoiseuilleInit q, float* wb) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < lxp * q.ly; i += gridDim.x * blockDim.x) {
+    const int x = i % lxp, y = i / lxp;
+    float b = 0.0f;
+    if (x < q.lx && mask[i] != kWall) {
+      const double dx = x - q.cx, dy = y - q.cy, s2 = (dx * dx + dy * dy) / (q.R * q.R);
+      b = float(-q.umax * fmax(0.0, 1.0 - s2));
+    }
+    wb[i] = b;
+  }
+}
+// Ghost columns of a periodic cross-section take their images' base.
+__global__ void wbase_ghosts_kernel(const int2* pairs, int n, float* wb) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    wb[pairs[i].x] = wb[pairs[i].y];
+}
+// The base's share of one step of the stored deviation s = w - wb (w's update is linear in the
+// corrector taps): wgt = tb Fz + K1 T1 + K2 T2 + (K0 - 1) wb, with T1 and T2 the base summed over
+// the six taps at distance 2 and 4 (the streamwise ones are the column's own base; outside the
+// cross-section the base is zero).
+__global__ void wgt_kernel(const float* wb, int lxp, int ly, float K0m1, float K1, float K2,
+                           float tfz, float* wgt) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < lxp * ly; i += gridDim.x * blockDim.x) {
+    const int x = i % lxp, y = i / lxp;
+    auto b = [&](int xx, int yy) {
+      return (xx < 0 || yy < 0 || xx >= lxp || yy >= ly) ? 0.0f : wb[yy * lxp + xx];
+    };
+    const float c = wb[i];
+    const float t1 = __fadd_rn(__fadd_rn(__fadd_rn(b(x - 2, y), b(x + 2, y)), __fadd_rn(b(x, y - 2), b(x, y + 2))),
+                               __fadd_rn(c, c));
+    const float t2 = __fadd_rn(__fadd_rn(__fadd_rn(b(x - 4, y), b(x + 4, y)), __fadd_rn(b(x, y - 4), b(x, y + 4))),
+                               __fadd_rn(c, c));
+    wgt[i] = __fmaf_rn(K1, t1, __fmaf_rn(K2, t2, __fmaf_rn(K0m1, c, tfz)));
+  }
+}
+
+cudaError_t launch_wbase_dense(const void* src, int src_is_f64, const uint8_t* mask, int lx, int lxp,
+                               int ly, int L, const int2* ghosts, int nghost, float* wb,
+                               cudaStream_t st) {
+  const int grid = std::max(1, std::min(592, (lxp * ly + 255) / 256));
+  if (src_is_f64) wbase_dense_kernel<double><<<grid, 256, 0, st>>>((const double*)src, mask, lx, lxp, ly, L, wb);
+  else wbase_dense_kernel<float><<<grid, 256, 0, st>>>((const float*)src, mask, lx, lxp, ly, L, wb);
+  if (nghost > 0) wbase_ghosts_kernel<<<std::min(592, (nghost + 255) / 256), 256, 0, st>>>(ghosts, nghost, wb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wbase_poiseuille(const uint8_t* mask, int lxp, const PoiseuilleInit& q,
+                                    const int2* ghosts, int nghost, float* wb, cudaStream_t st) {
+  const int grid = std::max(1, std::min(592, (lxp * q.ly + 255) / 256));
+  wbase_poiseuille_kernel<<<grid, 256, 0, st>>>(mask, lxp, q, wb);
+  if (nghost > 0) wbase_ghosts_kernel<<<std::min(592, (nghost + 255) / 256), 256, 0, st>>>(ghosts, nghost, wb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wgt(const float* wb, int lxp, int ly, float K0, float K1, float K2, float tfz,
+                       float* wgt, cudaStream_t st) {
+  const int grid = std::max(1, std::min(592, (lxp * ly + 255) / 256));
+  wgt_kernel<<<grid, 256, 0, st>>>(wb, lxp, ly, K0 - 1.0f, K1, K2, tfz, wgt);
   return cudaGetLastError();
 }
 

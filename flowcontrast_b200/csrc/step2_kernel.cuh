@@ -54,8 +54,14 @@ template <int D1, int TY, class TE = float> struct Step2Tile {
   static constexpr uint32_t TX_BYTES = uint32_t((SW * PH + 3 * UPLANE) * ES);
   static constexpr size_t RING_BYTES = size_t(S) * SLOT * ES;
   static constexpr size_t BAR_OFFSET = RING_BYTES;
+  // FP16 storage: the tile's base of w (FP32) for columns org.x-2 .. org.x+TX+1 and rows
+  // org.y-1 .. org.y+TY, after the barriers and counters
+  static constexpr int BW = TX + 4, BH = TY + 2;
+  static constexpr size_t BASE_OFFSET = (BAR_OFFSET + S * sizeof(uint64_t) + S * sizeof(uint32_t) + 15) / 16 * 16;
+  static constexpr size_t BASE_BYTES = std::is_same<TE, __half>::value ? size_t(BW) * BH * sizeof(float) : 0;
   // a "full" mbarrier per slot, then a release counter per slot
-  static constexpr size_t SMEM_BYTES = BAR_OFFSET + S * sizeof(uint64_t) + S * sizeof(uint32_t);
+  static constexpr size_t SMEM_BYTES = BASE_BYTES ? BASE_OFFSET + BASE_BYTES
+                                                  : BAR_OFFSET + S * sizeof(uint64_t) + S * sizeof(uint32_t);
   static_assert((PPLANE * ES) % 128 == 0 && (UPLANE * ES) % 16 == 0 && (SLOT * ES) % 128 == 0,
                 "TMA destinations must stay aligned");
   static_assert((HX * ES) % 16 == 0, "TMA box x start must be 16-byte aligned");
@@ -72,6 +78,10 @@ struct Step2Geom {
   unsigned* err;
   long long* step_counter;
   unsigned step_no;        // time step being computed (seed of the FP16 stochastic rounding)
+  // FP16 storage: stored w is w - wb (per-column base, FP32); wgt is the base's share of a step
+  // of the stored w. Null for other storage types.
+  const float* wb;
+  const float* wgt;
 };
 
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
@@ -227,6 +237,14 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
     }
     mbar_init_fence();
   }
+  // FP16 storage: the tile's base of w (zero outside the cross-section), read by the predictor
+  constexpr bool kBase = std::is_same<TE, __half>::value;
+  float* wbs = reinterpret_cast<float*>(smem + Tl::BASE_OFFSET);
+  if (kBase && g.wb)
+    for (int i = tid; i < Tl::BW * Tl::BH; i += Tl::THREADS) {
+      const int gx = org.x - 2 + i % Tl::BW, gy = org.y - 1 + i / Tl::BW;
+      wbs[i] = (gx >= 0 && gy >= 0 && gx < g.lxp && gy < g.ly) ? g.wb[size_t(gy) * g.lxp + gx] : 0.0f;
+    }
   __syncthreads();
 
   auto issue = [&](int m) {            // load march plane m into slot m % S
@@ -285,6 +303,8 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
   // the gauge may have been written by another CTA of the same (chained batched) launch: read
   // it from L2, not from a possibly stale L1 line
   const float gauge = g.gauge ? float(__ldcg(g.gauge)) : 0.0f;
+  const float2 wgt2 = (kBase && g.wgt && inside) ? *reinterpret_cast<const float2*>(g.wgt + size_t(y) * g.lxp + xa)
+                                                 : f2(0.f);
   const size_t FS = size_t(g.lxp) * g.ly * g.L;
   const TE* obase = reinterpret_cast<const TE*>(g.out);
   const uint32_t seed = hash32(g.step_no * 0x9e3779b9u + 0x632be5abu);
@@ -335,7 +355,14 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
       const float pc4[4] = {pL.y, pC.x, pC.y, pR.x};
       const float uc4[4] = {uL.y, uC.x, uC.y, uR.x};
       const float vc4[4] = {vL.y, vC.x, vC.y, vR.x};
-      const float wc4[4] = {wL.y, wC.x, wC.y, wR.x};
+      float wc4[4] = {wL.y, wC.x, wC.y, wR.x};
+      if (kBase && g.wb) {             // w = stored deviation + the column's base
+        const float* br = wbs + (ty + 1 + cy) * Tl::BW + 2 * tp;
+        const float2 bL = *reinterpret_cast<const float2*>(br), bC = *reinterpret_cast<const float2*>(br + 2),
+                     bR = *reinterpret_cast<const float2*>(br + 4);
+        wc4[0] = __fadd_rn(wc4[0], bL.y); wc4[1] = __fadd_rn(wc4[1], bC.x);
+        wc4[2] = __fadd_rn(wc4[2], bC.y); wc4[3] = __fadd_rn(wc4[3], bR.x);
+      }
       float q4[4], w24[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
@@ -451,7 +478,11 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
     const float2 dt = f2(k.dtddy), mm = f2(k.m), tb = f2(k.tb), cc = f2(k.cc);
     const float2 un = F::fma(F::add(F::fma(F::mul(dt, Lu), mm, us), f2(k.fx)), tb, F::mul(uc, cc));
     const float2 vn = F::fma(F::add(F::fma(F::mul(dt, Lv), mm, vs), f2(k.fy)), tb, F::mul(vc, cc));
-    const float2 wn = F::fma(F::add(F::fma(F::mul(dt, Lw), mm, wsz), f2(k.fz)), tb, F::mul(wc, cc));
+    // FP16 storage updates the stored deviation of w: the force's term becomes the column's base
+    // share of the step (tb fz included), see launch_wgt
+    const float2 wn = (kBase && g.wgt)
+        ? F::add(F::fma(F::fma(F::mul(dt, Lw), mm, wsz), tb, F::mul(wc, cc)), wgt2)
+        : F::fma(F::add(F::fma(F::mul(dt, Lw), mm, wsz), f2(k.fz)), tb, F::mul(wc, cc));
     if (inside) {   // wall columns get zero (fl = 0)
       PairStore<TE>::put(outp, FS, F::mul(rho, fl), F::mul(un, fl), F::mul(vn, fl),
                          F::mul(wn, fl), obase, seed);

@@ -76,7 +76,13 @@ template <class TE> struct Step4Tile {
   static constexpr uint32_t TX_BYTES = uint32_t((SW * PH + 3 * UPLANE) * ES);
   static constexpr size_t RING_BYTES = size_t(S) * SLOT * ES;
   static constexpr size_t BAR_OFFSET = RING_BYTES;
-  static constexpr size_t SMEM_BYTES = BAR_OFFSET + S * sizeof(uint64_t) + S * sizeof(uint32_t);
+  // FP16 storage: the tile's base of w (FP32) for columns org.x-4 .. org.x+TX+3 and rows
+  // org.y-1 .. org.y+TY, after the barriers and counters
+  static constexpr bool BASE = std::is_same<TE, __half>::value;
+  static constexpr int BW = TX + 8, BH = TY + 2;
+  static constexpr size_t BASE_OFFSET = (BAR_OFFSET + S * sizeof(uint64_t) + S * sizeof(uint32_t) + 15) / 16 * 16;
+  static constexpr size_t SMEM_BYTES = BASE ? BASE_OFFSET + size_t(BW) * BH * sizeof(float)
+                                            : BAR_OFFSET + S * sizeof(uint64_t) + S * sizeof(uint32_t);
   static_assert(S >= R + 2, "window too small for the corrector reach");
   static_assert((PPLANE * ES) % 128 == 0 && (UPLANE * ES) % 16 == 0 && (SLOT * ES) % 128 == 0,
                 "TMA destinations must stay aligned");
@@ -208,6 +214,15 @@ __device__ __forceinline__ bool step4_march(const CUtensorMap* tmap_p, const CUt
     }
     mbar_init_fence();
   }
+  // FP16 storage: the tile's base of w (zero outside the cross-section), read by the predictor
+  float* wbs = reinterpret_cast<float*>(smem + Tl::BASE_OFFSET);
+  if constexpr (Tl::BASE) {
+    if (g.wb)
+      for (int i = tid; i < Tl::BW * Tl::BH; i += Tl::THREADS) {
+        const int gx = org.x - 4 + i % Tl::BW, gy = org.y - 1 + i / Tl::BW;
+        wbs[i] = (gx >= 0 && gy >= 0 && gx < g.lxp && gy < g.ly) ? g.wb[size_t(gy) * g.lxp + gx] : 0.0f;
+      }
+  }
   __syncthreads();
 
   auto slot_of = [](int m) { return unsigned(m) % unsigned(S); };
@@ -325,6 +340,21 @@ __device__ __forceinline__ bool step4_march(const CUtensorMap* tmap_p, const CUt
       rowc(ss + uo + cy * SW, ur);
       rowc(ss + uo + UPL + cy * SW, vr);
       rowc(ss + uo + 2 * UPL + cy * SW, wr);
+      if constexpr (Tl::BASE) {        // w = stored deviation + the column's base
+        if (g.wb) {
+          const float* br = wbs + (ty + 1 + cy) * Tl::BW + 4 + C * tp;
+          float q[C];
+          ldv(br, q);
+          float l = __shfl_up_sync(0xffffffffu, q[C - 1], 1);
+          float r = __shfl_down_sync(0xffffffffu, q[0], 1);
+          if (edge_l) l = br[-1];
+          if (edge_r) r = br[C];
+          wr[0] = F::add(wr[0], l);
+#pragma unroll
+          for (int i = 0; i < C; ++i) wr[i + 1] = F::add(wr[i + 1], q[i]);
+          wr[C + 1] = F::add(wr[C + 1], r);
+        }
+      }
       T qr[C + 2], w2r[C + 2];
 #pragma unroll
       for (int j = 0; j < C + 2; ++j) {
@@ -460,7 +490,44 @@ __device__ __forceinline__ bool step4_march(const CUtensorMap* tmap_p, const CUt
     }
     field(0, uc, hu[H2], hu[ROT], mx, k.tb, k.tfx, res[1]);
     field(1, vc, hv[H2], hv[ROT], my, k.tb, k.tfy, res[2]);
-    field(2, wc, hw[H2], hw[ROT], comp[3], tbz, k.tfz, res[3]);
+    if constexpr (Tl::BASE) {          // the stored deviation of w: the column's base share
+      if (g.wgt) {
+        T tw[C];
+        if (inside) ldv(g.wgt + size_t(y) * g.lxp + xa, tw);
+        else for (int i = 0; i < C; ++i) tw[i] = T(0);
+        auto fieldw = [&](T (&out)[C]) {
+          const TE* q = so + uo + 2 * UPL;
+          T ext[C + 8];
+#pragma unroll
+          for (int v = 0; v < 4 / C; ++v) {
+            T a[C], b[C];
+            ldv(q - 4 + v * C, a);
+            ldv(q + C + v * C, b);
+#pragma unroll
+            for (int i = 0; i < C; ++i) { ext[v * C + i] = a[i]; ext[4 + C + v * C + i] = b[i]; }
+          }
+#pragma unroll
+          for (int i = 0; i < C; ++i) ext[4 + i] = wc[i];
+          T ym1[C], yp1[C], ym2[C], yp2[C], za1[C], za2[C];
+          ldv(q - D1 * SW, ym1); ldv(q + D1 * SW, yp1);
+          ldv(q - 2 * D1 * SW, ym2); ldv(q + 2 * D1 * SW, yp2);
+          ldv(sa1 + uo + 2 * UPL, za1); ldv(sa2 + uo + 2 * UPL, za2);
+#pragma unroll
+          for (int i = 0; i < C; ++i) {
+            const T t1 = F::add(F::add(F::add(ext[4 + i - D1], ext[4 + i + D1]), F::add(ym1[i], yp1[i])),
+                                F::add(hw[H2][i], za1[i]));
+            const T t2 = F::add(F::add(F::add(ext[i], ext[4 + i + 2 * D1]), F::add(ym2[i], yp2[i])),
+                                F::add(hw[ROT][i], za2[i]));
+            out[i] = F::fma(k.K1, t1, F::fma(k.K2, t2, F::fma(k.K0, wc[i], F::fma(tbz, comp[3][i], tw[i]))));
+          }
+        };
+        fieldw(res[3]);
+      } else {
+        field(2, wc, hw[H2], hw[ROT], comp[3], tbz, k.tfz, res[3]);
+      }
+    } else {
+      field(2, wc, hw[H2], hw[ROT], comp[3], tbz, k.tfz, res[3]);
+    }
 #pragma unroll
     for (int i = 0; i < C; ++i) { hu[ROT][i] = uc[i]; hv[ROT][i] = vc[i]; hw[ROT][i] = wc[i]; }
     if (inside) {   // wall and padding columns get zero (fl = 0)
