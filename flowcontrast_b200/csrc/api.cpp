@@ -204,7 +204,7 @@ struct fslbm_solve {
   CUtensorMap maps[2];
   // FP32 column-pair kernel (even d1): tile height, persistent grid, two maps per buffer
   bool use2 = false;
-  int ty2 = 32, grid2 = 0, packed2 = 1, cols2 = 4;
+  int ty2 = 32, grid2 = 0, packed2 = 1;
   std::vector<int> tile_warps[2];  // per column-pair tile: warps holding fluid, [0] 32 x 2, [1] 16 x 4
   CUtensorMap maps2p[2], maps2u[2];
   DevCounters* d_counters = nullptr;
@@ -328,10 +328,8 @@ static std::vector<int2> fluid_tiles(const fslbm_solve* s, int th) {
 static void choose_chunks(fslbm_solve* s);
 
 // Selects the step kernel for the current dtype and d1, uploads its tile list, builds its
-// tensor maps and sizes its grid. For comparisons: FSLBM_STEP_KERNEL=1 forces the one-column
-// kernel, FSLBM_STEP_COLS=2 the FP32/FP16 column-pair kernel instead of the four-column march
-// (FSLBM_PACKED=0: its scalar pair arithmetic; FSLBM_TILE_Y=16: its 32 x 16 tiles). Batched
-// launches always run the four-column march; FP64 runs the two-column march on 32 x 16 tiles.
+// tensor maps and sizes its grid. FSLBM_STEP_KERNEL=1 forces the one-column kernel and
+// FSLBM_PACKED=0 uses scalar pair arithmetic and FSLBM_TILE_Y=16|32 picks the column-pair kernel's tile height (for comparisons).
 static int configure_kernel(fslbm_solve* s) {
   const char* ek = std::getenv("FSLBM_STEP_KERNEL");
   const char* et = std::getenv("FSLBM_TILE_Y");
@@ -340,23 +338,19 @@ static int configure_kernel(fslbm_solve* s) {
   // FP16 storage exists only in the column-pair kernel, which has the 2-tap corrector
   s->use2 = step2_supported(s->dtype, s->prm.d1) && s->K == 2 && s->planes == 1 &&
             (s->dtype == FSLBM_F16 || !(ek && std::atoi(ek) == 1));
-  s->ty2 = s->dtype == FSLBM_F64 ? 16 : (et && std::atoi(et) == 16) ? 16 : 32;
+  s->ty2 = (et && std::atoi(et) == 16) ? 16 : 32;
   const char* ep = std::getenv("FSLBM_PACKED");
   s->packed2 = (ep && std::atoi(ep) == 0) ? 0 : 1;
-  const char* ec = std::getenv("FSLBM_STEP_COLS");
-  s->cols2 = (ec && std::atoi(ec) == 2) || s->ty2 != 32 ? 2 : 4;
   const std::vector<int2> tiles = fluid_tiles(s, s->use2 ? s->ty2 : kTY);
   s->tile_warps[0].clear();
   s->tile_warps[1].clear();
-  // computing warps per tile of the four-column march (8 warps of 32 x 4 or 16 x 8 cells), the
-  // cost of a batched work item
   if (s->use2)
     for (const int2 org : tiles)
       for (int shape = 0; shape < 2; ++shape) {
-        const int wx = shape ? 16 : 32, wy = shape ? 8 : 4;
+        const int wx = shape ? 16 : 32, wy = shape ? 4 : 2;
         int warps = 0;
-        for (int w = 0; w < 8; ++w) {
-          const int x0 = org.x + (shape ? 16 * (w & 1) : 0), y0 = org.y + (shape ? 8 * (w >> 1) : 4 * w);
+        for (int w = 0; w < s->ty2 / 2; ++w) {
+          const int x0 = org.x + (shape ? 16 * (w & 1) : 0), y0 = org.y + (shape ? 4 * (w >> 1) : 2 * w);
           bool any = false;
           for (int y = y0; y < std::min(y0 + wy, s->ly) && !any; ++y)
             for (int x = x0; x < std::min(x0 + wx, s->lxp) && !any; ++x)
@@ -702,8 +696,9 @@ static int update_wgt(fslbm_solve* s) {
   if (!s->d_wgt) return FSLBM_OK;
   StepLaunch a{};
   fill_constants(s, a);
-  const float tb = float(a.tb), am = tb * float(a.dtddy) * float(a.m);
-  const float K0 = am * float(a.c0) + float(a.cc), K1 = am * float(a.c1), K2 = am * float(a.c2);
+  // the step kernel's folded constants, formed the same way (FP32, K0 with one fused rounding)
+  const float tb = float(a.tb), am = (tb * float(a.dtddy)) * float(a.m);
+  const float K0 = std::fmaf(am, float(a.c0), float(a.cc)), K1 = am * float(a.c1), K2 = am * float(a.c2);
   CUDA_TRY(launch_wgt(s->d_wbase, s->lxp, s->ly, K0, K1, K2, tb * float(a.fz), s->d_wgt,
                       s->ctx->stream));
   return FSLBM_OK;
@@ -924,8 +919,7 @@ static int enqueue_steps(fslbm_solve* s, int64_t nsteps) {
       CUDA_TRY(cudaEventRecord(s->tev[s->tev_used], st));
     }
     if (s->use2) {
-      Step2Launch b2{s->prm.d1, s->ty2, s->packed2, &s->maps2p[s->cur], &s->maps2u[s->cur], s->grid2,
-                     s->cols2};
+      Step2Launch b2{s->prm.d1, s->ty2, s->packed2, &s->maps2p[s->cur], &s->maps2u[s->cur], s->grid2};
       CUDA_TRY(launch_step2(a, b2, st));
     } else {
       CUDA_TRY(launch_step(a, st));
@@ -1312,7 +1306,7 @@ static void free_batch(fslbm_batch* b) {
 // marched (the chunk plus the 2R pipeline planes) times the tile's warps that compute plus two
 // for the pipeline's fixed cost.
 static int64_t item_cost(const fslbm_solve* s, int tile, int nout, int w16x4) {
-  return int64_t(nout + 4 * s->prm.d1) * (s->tile_warps[w16x4 ? 1 : 0][tile] + 1);
+  return int64_t(nout + 4 * s->prm.d1) * (s->tile_warps[w16x4 ? 1 : 0][tile] + 2);
 }
 
 // Streamwise chunks of a member: about `chunk` planes each, at least 4*d1 planes.

@@ -61,16 +61,12 @@ cudaError_t launch_step(const StepLaunch& a, cudaStream_t st);
 
 // FP32 column-pair kernel (even d1): two tensor maps per input state (p box with a one-cell
 // halo, u,v,w box with the corrector halo) and a persistent grid.
-// The same boxes feed the multi-column march (step4_kernel.cuh: four columns per thread on
-// 32 x 32 tiles for FP32/FP16, two columns on 32 x 16 tiles for FP64), which is the default;
-// cols = 2 selects the FP32/FP16 column-pair kernel (kept for comparisons).
 struct Step2Launch {
   int d1, ty;                // corrective stride, tile height (16 or 32)
-  int packed;                // column pairs: FP32x2 packed arithmetic (1) or scalar pairs (0)
+  int packed;                // FP32x2 packed arithmetic (1) or scalar pairs (0)
   const CUtensorMap* map_p;
   const CUtensorMap* map_uvw;
   int grid;
-  int cols = 4;              // FP32/FP16 columns per thread: 4 (tile height 32) or 2
 };
 bool step2_supported(int dtype, int d1);
 bool step2_box(int dtype, int d1, int ty, int* sw, int* ph, int* uh, int* hx, int* hy);

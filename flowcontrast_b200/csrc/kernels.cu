@@ -6,7 +6,6 @@
 #include "internal.h"
 #include "step_kernel.cuh"
 #include "step2_kernel.cuh"
-#include "step4_kernel.cuh"
 
 namespace fslbm {
 
@@ -101,7 +100,7 @@ cudaError_t launch_step(const StepLaunch& a, cudaStream_t st) {
 // FP32 column-pair kernel dispatch
 // ------------------------------------------------------------------------------------------
 bool step2_supported(int dtype, int d1) {
-  return (dtype == FSLBM_F32 || dtype == FSLBM_F16 || dtype == FSLBM_F64) && d1 == 2;
+  return (dtype == FSLBM_F32 || dtype == FSLBM_F16) && d1 == 2;
 }
 
 template <int TY, class TE> static void box2(int* sw, int* ph, int* uh, int* hx, int* hy) {
@@ -111,12 +110,6 @@ template <int TY, class TE> static void box2(int* sw, int* ph, int* uh, int* hx,
 
 bool step2_box(int dtype, int d1, int ty, int* sw, int* ph, int* uh, int* hx, int* hy) {
   if (d1 != 2 || (ty != 32 && ty != 16)) return false;
-  if (dtype == FSLBM_F64) {            // the multi-column march's FP64 tiles (32 x 16)
-    using Tl = Step4Tile<double>;
-    if (ty != Tl::TY) return false;
-    *sw = Tl::SW; *ph = Tl::PH; *uh = Tl::UH; *hx = Tl::HX; *hy = Tl::HY;
-    return true;
-  }
   if (dtype == FSLBM_F32) {
     if (ty == 32) box2<32, float>(sw, ph, uh, hx, hy);
     else box2<16, float>(sw, ph, uh, hx, hy);
@@ -151,23 +144,10 @@ template <class TE> static cudaError_t prep2_all(int ty) {
   return cudaErrorInvalidValue;
 }
 
-template <class TE> static cudaError_t prep4() {
-  return cudaFuncSetAttribute(fslbm_step4_kernel<TE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(Step4Tile<TE>::SMEM_BYTES));
-}
-
 cudaError_t step2_prepare(int dtype, int d1, int ty) {
   if (d1 != 2) return cudaErrorInvalidValue;
-  if (dtype == FSLBM_F64) return ty == Step4Tile<double>::TY ? prep4<double>() : cudaErrorInvalidValue;
-  cudaError_t e;
-  if (dtype == FSLBM_F32) {
-    if ((e = prep4<float>())) return e;
-    return prep2_all<float>(ty);
-  }
-  if (dtype == FSLBM_F16) {
-    if ((e = prep4<__half>())) return e;
-    return prep2_all<__half>(ty);
-  }
+  if (dtype == FSLBM_F32) return prep2_all<float>(ty);
+  if (dtype == FSLBM_F16) return prep2_all<__half>(ty);
   return cudaErrorInvalidValue;
 }
 
@@ -187,16 +167,6 @@ static cudaError_t launch_step2_t(const Step2Launch& b, const Step2Geom& g,
   return cudaGetLastError();
 }
 
-template <class TE, class T>
-static cudaError_t launch_step4_t(const Step2Launch& b, const Step2Geom& g, const StepConst<T>& k,
-                                  cudaStream_t st) {
-  using Tl = Step4Tile<TE>;
-  if (b.ty != Tl::TY) return cudaErrorInvalidValue;
-  fslbm_step4_kernel<TE><<<b.grid, Tl::THREADS, Tl::SMEM_BYTES, st>>>(*b.map_p, *b.map_uvw, g,
-                                                                      step4_const(k));
-  return cudaGetLastError();
-}
-
 cudaError_t launch_step2(const StepLaunch& a, const Step2Launch& b, cudaStream_t st) {
   Step2Geom g;
   g.lxp = a.lxp; g.ly = a.ly; g.L = a.L; g.ntiles = a.ntiles; g.nchunks = b.grid / a.ntiles;
@@ -211,17 +181,6 @@ cudaError_t launch_step2(const StepLaunch& a, const Step2Launch& b, cudaStream_t
   k.m = float(a.m); k.c0 = float(a.c0); k.c1 = float(a.c1); k.c2 = float(a.c2);
   k.fx = float(a.fx); k.fy = float(a.fy); k.fz = float(a.fz);
   if (b.d1 != 2) return cudaErrorInvalidValue;
-  if (a.dtype == FSLBM_F64) {          // two columns per thread, FP64 arithmetic, 32 x 16 tiles
-    StepConst<double> kd;
-    kd.tb = a.tb; kd.cc = a.cc; kd.pin = a.pin; kd.dtddy = a.dtddy; kd.m = a.m;
-    kd.c0 = a.c0; kd.c1 = a.c1; kd.c2 = a.c2; kd.fx = a.fx; kd.fy = a.fy; kd.fz = a.fz;
-    return launch_step4_t<double>(b, g, kd, st);
-  }
-  if (b.cols != 2) {                   // four columns per thread, 32 x 32 tiles
-    if (a.dtype == FSLBM_F32) return launch_step4_t<float>(b, g, k, st);
-    if (a.dtype == FSLBM_F16) return launch_step4_t<__half>(b, g, k, st);
-    return cudaErrorInvalidValue;
-  }
   if (a.dtype == FSLBM_F32) return launch_step2_t<float>(b, g, k, st);
   if (a.dtype == FSLBM_F16) return launch_step2_t<__half>(b, g, k, st);
   return cudaErrorInvalidValue;
@@ -300,7 +259,7 @@ __global__ void monitor_kernel(MonitorLaunch a) {
 struct alignas(64) BatchMember {
   CUtensorMap map_p[2], map_u[2];
   Step2Geom g;                 // g.out is replaced by the buffer the step writes
-  Step4Const<float> k;
+  StepConst<float> k;
   void* state[2];
   const double* gauge_slot;    // the member's monitor p2, applied on the step after a monitor
   const long long* steps;      // the member's device step counter
@@ -338,7 +297,7 @@ __device__ __forceinline__ void batch_book(const BatchMon& b, int parity_after, 
 // False when the wait gave up (error flag set). Inlined for the same reason as batch_book.
 __device__ __forceinline__ bool batch_item_begin(const BatchMember& mb, int member, int step,
                                               const unsigned* sync, unsigned* err, Step2Geom* s_g,
-                                              Step4Const<float>* s_k, long long* s_done) {
+                                              StepConst<float>* s_k, long long* s_done) {
   if (step > 0 && !wait_geq_gpu(sync + 5 + 2 * member, unsigned(step), kWaitLimitNs)) {
     atomicOr(err, 1u);
     return false;
@@ -375,7 +334,7 @@ __device__ __forceinline__ bool batch_item_begin(const BatchMember& mb, int memb
 // and releases it before marching on. Counting there rather than right after the march keeps
 // the march free of register spills.
 template <int D1, int TY, bool PK, class TE>
-__global__ void __launch_bounds__(Step4Tile<TE>::THREADS, 1)
+__global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
     fslbm_step2_batch_kernel(const BatchMember* __restrict__ members,
                              const BatchMon* __restrict__ mons, const int2* __restrict__ items,
                              int nitems, int nsteps, unsigned* sync, unsigned* err) {
@@ -386,7 +345,7 @@ __global__ void __launch_bounds__(Step4Tile<TE>::THREADS, 1)
   __shared__ double s_sh[3 * 32];
   // the item's geometry and constants, read by the march from shared memory (the single-pipe
   // kernel reads them from the parameter bank); kept in registers through the march they spill
-  __shared__ Step4Const<float> s_k;
+  __shared__ StepConst<float> s_k;
   __shared__ Step2Geom s_g;
   bool first = true;
   unsigned prev = ~0u;             // the CTA's previous ticket, counted at the next claim
@@ -429,10 +388,12 @@ __global__ void __launch_bounds__(Step4Tile<TE>::THREADS, 1)
       const int cur = mb.cur0 ^ (step & 1);
       const int ntiles = mb.g.ntiles;
       // the warp shape is a compile-time choice (a runtime one raises register pressure)
-      const bool ok = mb.w16x4 ? step4_march<TE, true>(&mb.map_p[cur], &mb.map_u[cur], s_g, s_k,
-                                                       it.y % ntiles, it.y / ntiles, smem, !first)
-                               : step4_march<TE, false>(&mb.map_p[cur], &mb.map_u[cur], s_g, s_k,
-                                                        it.y % ntiles, it.y / ntiles, smem, !first);
+      const bool ok = mb.w16x4 ? step2_march<D1, TY, PK, TE, true>(&mb.map_p[cur], &mb.map_u[cur], s_g,
+                                                                   s_k, it.y % ntiles, it.y / ntiles,
+                                                                   smem, !first)
+                               : step2_march<D1, TY, PK, TE, false>(&mb.map_p[cur], &mb.map_u[cur], s_g,
+                                                                    s_k, it.y % ntiles, it.y / ntiles,
+                                                                    smem, !first);
       if (!ok) return;
       first = false;
     }
@@ -442,12 +403,19 @@ __global__ void __launch_bounds__(Step4Tile<TE>::THREADS, 1)
 template <bool PK, class TE> static cudaError_t batch_prep() {
   return cudaFuncSetAttribute(fslbm_step2_batch_kernel<2, 32, PK, TE>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(Step4Tile<TE>::SMEM_BYTES));
+                              int(Step2Tile<2, 32, TE>::SMEM_BYTES));
 }
 
 cudaError_t batch_prepare(int dtype) {
-  if (dtype == FSLBM_F32) return batch_prep<false, float>();
-  if (dtype == FSLBM_F16) return batch_prep<false, __half>();
+  cudaError_t e;
+  if (dtype == FSLBM_F32) {
+    if ((e = batch_prep<true, float>())) return e;
+    return batch_prep<false, float>();
+  }
+  if (dtype == FSLBM_F16) {
+    if ((e = batch_prep<true, __half>())) return e;
+    return batch_prep<false, __half>();
+  }
   return cudaErrorInvalidValue;
 }
 
@@ -465,11 +433,9 @@ cudaError_t fill_batch_member(void* dst, const CUtensorMap* mp, const CUtensorMa
   m.g.tiles = a.tiles; m.g.mask = a.mask; m.g.colcoef = a.colcoef; m.g.out = nullptr;
   m.g.gauge = nullptr; m.g.err = a.err; m.g.step_counter = nullptr; m.g.step_no = 0;
   m.g.wb = a.wb; m.g.wgt = a.wgt;
-  StepConst<float> k;
-  k.tb = float(a.tb); k.cc = float(a.cc); k.pin = float(a.pin); k.dtddy = float(a.dtddy);
-  k.m = float(a.m); k.c0 = float(a.c0); k.c1 = float(a.c1); k.c2 = float(a.c2);
-  k.fx = float(a.fx); k.fy = float(a.fy); k.fz = float(a.fz);
-  m.k = step4_const(k);
+  m.k.tb = float(a.tb); m.k.cc = float(a.cc); m.k.pin = float(a.pin); m.k.dtddy = float(a.dtddy);
+  m.k.m = float(a.m); m.k.c0 = float(a.c0); m.k.c1 = float(a.c1); m.k.c2 = float(a.c2);
+  m.k.fx = float(a.fx); m.k.fy = float(a.fy); m.k.fz = float(a.fz);
   m.state[0] = state0; m.state[1] = state1;
   m.gauge_slot = gauge_slot; m.steps = steps; m.stop_at = stop_at; m.w16x4 = w16x4;
   m.monitor_every = monitor_every; m.cur0 = cur0;
@@ -481,10 +447,13 @@ template <class TE>
 static void launch_batch_t(const BatchMember* mb, const BatchMon* mons, const int2* items,
                            int nitems, int nsteps, int grid, int packed, unsigned* sync,
                            unsigned* err, cudaStream_t st) {
-  using Tl = Step4Tile<TE>;
-  (void)packed;
-  fslbm_step2_batch_kernel<2, 32, false, TE><<<grid, Tl::THREADS, Tl::SMEM_BYTES, st>>>(
-      mb, mons, items, nitems, nsteps, sync, err);
+  using Tl = Step2Tile<2, 32, TE>;
+  if (packed)
+    fslbm_step2_batch_kernel<2, 32, true, TE><<<grid, Tl::THREADS, Tl::SMEM_BYTES, st>>>(
+        mb, mons, items, nitems, nsteps, sync, err);
+  else
+    fslbm_step2_batch_kernel<2, 32, false, TE><<<grid, Tl::THREADS, Tl::SMEM_BYTES, st>>>(
+        mb, mons, items, nitems, nsteps, sync, err);
 }
 
 size_t batch_sync_words(int nmembers) { return 4 + 2 * size_t(nmembers); }

@@ -318,6 +318,11 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
   const float nx[2] = {-36.f * wsx.x, -36.f * wsx.y};
   const float ny[2] = {-36.f * wsy.x, -36.f * wsy.y};
   const float h6 = float(dir) / 72.0f;
+  // folded update: u_new = K1 t1 + K2 t2 + K0 u + tb (u* + F), the corrector's taps t1 / t2 at
+  // distance d1 / 2 d1, K0 = tb dtddy m c0 + (1 - tb), K1 = tb dtddy m c1, K2 = tb dtddy m c2
+  const float kam = __fmul_rn(__fmul_rn(k.tb, k.dtddy), k.m);
+  const float kK0 = __fmaf_rn(kam, k.c0, k.cc), kK1 = __fmul_rn(kam, k.c1), kK2 = __fmul_rn(kam, k.c2);
+  const float ktz = __fmul_rn(float(dir), k.tb);              // the z-moment carries the sign
 
   float2 hu[4], hv[4], hw[4];                                 // own columns of planes jo-4..jo-1
   // Predictor terms waiting for their output plane: b2 = the march-previous plane's share of the
@@ -409,28 +414,34 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
     // e + h (next), (2/3) A0 (self) and e - h (previous); for the z-moment h - e (previous),
     // none (self) and e + h (next), times dir.
     float cmp[4][2];
+    if (sp < 0 || sp >= g.L) {         // seam plane (CTA-uniform): the pressure jump's share
+#pragma unroll
+      for (int col = 0; col < 2; ++col) {
+        A[col][0] = __fmaf_rn(off, n0[col], A[col][0]);
+        X[col][0] = __fmaf_rn(off, nx[col], X[col][0]);
+        Y[col][0] = __fmaf_rn(off, ny[col], Y[col][0]);
+      }
+    }
 #pragma unroll
     for (int col = 0; col < 2; ++col) {
-      const float A0 = __fmaf_rn(off, n0[col], A[col][0]);
-      const float X0 = __fmaf_rn(off, nx[col], X[col][0]);
-      const float Y0 = __fmaf_rn(off, ny[col], Y[col][0]);
-      const float eA = __fmaf_rn(A[col][2], 1.0f / 48.0f, A0 * (1.0f / 216.0f));
-      const float hA = A[col][1] * h6;
-      const float eX = __fmaf_rn(X[col][2], 1.0f / 48.0f, X0 * (1.0f / 216.0f));
-      const float hX = X[col][1] * h6;
-      const float eY = __fmaf_rn(Y[col][2], 1.0f / 48.0f, Y0 * (1.0f / 216.0f));
-      const float hY = Y[col][1] * h6;
-      const float sA = eA + hA;
-      cmp[0][col] = __fmaf_rn(s1[0][col], 1.0f / 54.0f, b2[0][col] + sA);
-      cmp[1][col] = __fmaf_rn(s1[1][col], 1.0f / 54.0f, b2[1][col] + (eX + hX));
-      cmp[2][col] = __fmaf_rn(s1[2][col], 1.0f / 54.0f, b2[2][col] + (eY + hY));
-      cmp[3][col] = b2[3][col] + sA;
+      const float A0 = A[col][0], X0 = X[col][0], Y0 = Y[col][0];
+      const float eA = __fmaf_rn(A[col][2], 1.0f / 48.0f, __fmul_rn(A0, 1.0f / 216.0f));
+      const float eX = __fmaf_rn(X[col][2], 1.0f / 48.0f, __fmul_rn(X0, 1.0f / 216.0f));
+      const float eY = __fmaf_rn(Y[col][2], 1.0f / 48.0f, __fmul_rn(Y0, 1.0f / 216.0f));
+      // e + h and e - h with h = A1 h6, each one fused rounding
+      const float sA = __fmaf_rn(A[col][1], h6, eA), dA = __fmaf_rn(A[col][1], -h6, eA);
+      const float sX = __fmaf_rn(X[col][1], h6, eX), dX = __fmaf_rn(X[col][1], -h6, eX);
+      const float sY = __fmaf_rn(Y[col][1], h6, eY), dY = __fmaf_rn(Y[col][1], -h6, eY);
+      cmp[0][col] = __fmaf_rn(s1[0][col], 1.0f / 54.0f, __fadd_rn(b2[0][col], sA));
+      cmp[1][col] = __fmaf_rn(s1[1][col], 1.0f / 54.0f, __fadd_rn(b2[1][col], sX));
+      cmp[2][col] = __fmaf_rn(s1[2][col], 1.0f / 54.0f, __fadd_rn(b2[2][col], sY));
+      cmp[3][col] = __fadd_rn(b2[3][col], sA);
 #pragma unroll
       for (int q = 0; q < 4; ++q) b2[q][col] = b1[q][col];
-      b1[0][col] = eA - hA;
-      b1[1][col] = eX - hX;
-      b1[2][col] = eY - hY;
-      b1[3][col] = hA - eA;
+      b1[0][col] = dA;
+      b1[1][col] = dX;
+      b1[2][col] = dY;
+      b1[3][col] = -dA;
       s1[0][col] = A0;
       s1[1][col] = X0;
       s1[2][col] = Y0;
@@ -456,7 +467,8 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
     const TE* sa2 = ring + ((jo + 2 * D1) & (S - 1)) * SLOT;
     const float2 pc = lds2(so + po);
     const float2 uc = lds2(so + uo), vc = lds2(so + uo + UPL), wc = lds2(so + uo + 2 * UPL);
-    auto lap = [&](int f, float2 c, float2 zb1, float2 zb2) {
+    // u_new = K1 t1 + K2 t2 + K0 u + tb m* + tb F
+    auto update = [&](int f, float2 c, float2 zb1, float2 zb2, float2 mom, float tm, float2 tf) {
       const TE* q = so + uo + f * UPL;
       const float2 za1 = lds2(sa1 + uo + f * UPL), za2 = lds2(sa2 + uo + f * UPL);
       const float2 t1 = F::add(F::add(F::add(lds2(q - D1), lds2(q + D1)),
@@ -465,27 +477,24 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
       const float2 t2 = F::add(F::add(F::add(lds2(q - 2 * D1), lds2(q + 2 * D1)),
                                       F::add(lds2(q - 2 * D1 * SW), lds2(q + 2 * D1 * SW))),
                                F::add(zb2, za2));
-      return F::fma(f2(k.c2), t2, F::fma(f2(k.c1), t1, F::mul(f2(k.c0), c)));
+      return F::fma(f2(kK1), t1, F::fma(f2(kK2), t2, F::fma(f2(kK0), c, F::fma(f2(tm), mom, tf))));
     };
     constexpr int H2 = (ROT + 2) & 3;                         // plane jo-2
-    const float2 Lu = lap(0, uc, hu[H2], hu[ROT]);
-    const float2 Lv = lap(1, vc, hv[H2], hv[ROT]);
-    const float2 Lw = lap(2, wc, hw[H2], hw[ROT]);
-    hu[ROT] = uc; hv[ROT] = vc; hw[ROT] = wc;
     const float2 rho = F::add(F::fma(pc, ws0, comp0), f2(-gauge));
     const float2 us = F::fma(pc, wsx, comp1), vs = F::fma(pc, wsy, comp2);
-    const float2 wsz = F::mul(comp3, f2(float(dir)));
-    const float2 dt = f2(k.dtddy), mm = f2(k.m), tb = f2(k.tb), cc = f2(k.cc);
-    const float2 un = F::fma(F::add(F::fma(F::mul(dt, Lu), mm, us), f2(k.fx)), tb, F::mul(uc, cc));
-    const float2 vn = F::fma(F::add(F::fma(F::mul(dt, Lv), mm, vs), f2(k.fy)), tb, F::mul(vc, cc));
-    // FP16 storage updates the stored deviation of w: the force's term becomes the column's base
-    // share of the step (tb fz included), see launch_wgt
-    const float2 wn = (kBase && g.wgt)
-        ? F::add(F::fma(F::fma(F::mul(dt, Lw), mm, wsz), tb, F::mul(wc, cc)), wgt2)
-        : F::fma(F::add(F::fma(F::mul(dt, Lw), mm, wsz), f2(k.fz)), tb, F::mul(wc, cc));
+    const float2 un = update(0, uc, hu[H2], hu[ROT], us, k.tb, f2(__fmul_rn(k.tb, k.fx)));
+    const float2 vn = update(1, vc, hv[H2], hv[ROT], vs, k.tb, f2(__fmul_rn(k.tb, k.fy)));
+    // FP16 storage updates the stored deviation of w: the force's term becomes the column's share
+    // of the step of the base (tb fz included), see launch_wgt
+    const float2 wn = update(2, wc, hw[H2], hw[ROT], comp3, ktz,
+                             (kBase && g.wgt) ? wgt2 : f2(__fmul_rn(k.tb, k.fz)));
+    hu[ROT] = uc; hv[ROT] = vc; hw[ROT] = wc;
     if (inside) {   // wall columns get zero (fl = 0)
-      PairStore<TE>::put(outp, FS, F::mul(rho, fl), F::mul(un, fl), F::mul(vn, fl),
-                         F::mul(wn, fl), obase, seed);
+      if (fl.x != 0.f && fl.y != 0.f)
+        PairStore<TE>::put(outp, FS, rho, un, vn, wn, obase, seed);
+      else
+        PairStore<TE>::put(outp, FS, F::mul(rho, fl), F::mul(un, fl), F::mul(vn, fl),
+                           F::mul(wn, fl), obase, seed);
     }
     outp += ostep;
   };

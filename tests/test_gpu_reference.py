@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import ref_cases as RC
-from test_oracle_golden import GAUGE_TOL, TOL, gauge_offset, load, rel
+from test_oracle_golden import GAUGE_TOL, gauge_offset, load, rel, tol
 
 pytestmark = pytest.mark.gpu
 
@@ -36,7 +36,7 @@ def test_gpu_matches_reference_kernels(built, ctx, name):
             got = out.reshape(4, -1)[:, keep].astype(np.float64)
             got[0] -= gauge_offset(g, c, n, [m["p2"] for m in mons])
             ep, eu = rel(got, g[f"step{n}"].astype(np.float64))
-            assert ep < TOL and eu < TOL, (name, dt, n, ep, eu)
+            assert ep < tol(n) and eu < tol(n), (name, dt, n, ep, eu)
             if f"p2_step{n}" in g:
                 want = g[f"p2_step{n}"].astype(np.float64)
                 p2 = np.array([m["p2"] for m in mons])

@@ -7,8 +7,9 @@ buffer plane (FSLBM.cu:630-647) is subtracted from p in step 51 (FSLBM.cu:628, 2
 oracle's monitor forms that p2 in FP64, the reference's harness in FP32 as the reference does.
 
 Tolerance: relative L2 over non-wall cells of the reference layout, separately for u=(u,v,w)
-and for p scaled by |p| + 1.5|u|^2: 2e-6 (both sides compute in FP32 with different operation
-order; FP32-vs-FP64 drift of the method itself is ~1e-6 over 40 steps on these cases). The
+and for p scaled by |p| + 1.5|u|^2: 2e-6 up to 40 steps, growing in proportion beyond (both
+sides compute in FP32 with different operation order, and their rounding differences grow with
+the step count: FP32-vs-FP64 drift of the method itself is ~1e-6 over 40 steps). The
 gauges agree to 1e-4 relative: the reference forms the cell count l1 by adding 1/(2 d2) in FP32
 once per buffer cell (FSLBM.cu:589-591), about 2300 additions of an inexact 0.05 here, which
 leaves it about 2e-5 off the exact count the oracle and the solver use. A gauge shifts p by
@@ -29,6 +30,11 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 TOL = 2e-6
 GAUGE_TOL = 1e-4
+
+
+def tol(n):
+    """FP32-against-FP32 tolerance after n steps."""
+    return TOL * max(1.0, n / 40.0)
 
 
 def load(name):
@@ -78,7 +84,7 @@ def test_oracle_matches_reference_kernels(name, dtype):
         got[0] -= gauge_offset(g, c, n, gauges)
         want = g[f"step{n}"].astype(np.float64)
         ep, eu = rel(got, want)
-        assert ep < TOL and eu < TOL, (name, n, ep, eu)
+        assert ep < tol(n) and eu < tol(n), (name, n, ep, eu)
         if f"p2_step{n}" in g:
             want_p2 = g[f"p2_step{n}"].astype(np.float64)
             assert len(want_p2) == len(gauges) and np.all(np.abs(want_p2) > 0)
