@@ -96,13 +96,17 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x) {
   return x;
 }
 
-// FP32 -> FP16 with stochastic rounding: uniform noise below FP16's last kept mantissa bit
-// (the low 13 bits of an FP32 of FP16's normal range) is added to the magnitude, which is then
-// truncated. The result is unbiased, so increments far below half an FP16 ulp (the body force
-// and the slow relaxation of the step) survive in expectation instead of being rounded away.
-// In FP16's subnormal range the noise covers only part of the dropped bits (error < 2^-24).
+// FP32 -> FP16 with stochastic rounding: uniform noise below FP16's last kept bit is added to
+// the magnitude, which is then truncated. The result is unbiased, so increments far below half
+// an FP16 ulp (the body force and the slow relaxation of the step) survive in expectation
+// instead of being rounded away. In FP16's normal range the kept bit is the 11th of the
+// significand, so the noise is the low 13 bits of the FP32 pattern; below 2^-14 (FP16
+// subnormals, which the deviations of FP16 storage often reach) it is fixed at 2^-24 and the
+// noise is scaled to it.
 __device__ __forceinline__ __half sr_half(float x, uint32_t r) {
-  return __float2half_rz(__uint_as_float(__float_as_uint(x) + (r & 0x1fffu)));
+  if (fabsf(x) >= 6.103515625e-05f)
+    return __float2half_rz(__uint_as_float(__float_as_uint(x) + (r & 0x1fffu)));
+  return __float2half_rz(x + copysignf(float(r & 0x1fffu) * (5.9604644775390625e-08f / 8192.0f), x));
 }
 
 // Stores of one column pair's four fields. FP32 storage stores the values; FP16 storage rounds

@@ -1,7 +1,10 @@
 """FP16 storage with FP32 arithmetic (dtype F16) against the oracle.
 
 The FP16 form computes each step in FP32 exactly as the FP32 form does and rounds the four
-stored fields stochastically to FP16 (unbiased; noise seeded by cell and step only).
+stored fields stochastically to FP16 (unbiased; noise seeded by cell and step only). p, u and
+v are stored as they are (p is already the deviation rho - 1 from rest); w is stored as the
+deviation from a per-column FP32 base (the streamwise mean of the fields it was given), so its
+rounding is relative to the flow's departure from that profile, not to the profile itself.
 Stated tolerances:
   one step from an FP16-exact state: every stored value within one FP16 ulp (plus 2e-7, the
     FP32 reassociation of pressure's O(0.1) terms) of the FP32 oracle's value (stochastic
@@ -11,8 +14,10 @@ Stated tolerances:
     drift the FP16 core-mean change matches the FP32 change within 5 % (round-to-nearest
     storage would keep it at zero);
   200 steps of the small Poiseuille pipe (64 x 32 x 32, Re 100): relative L2 error of u and of
-    p (scaled as in the FP32 parity tests) <= 3e-3 against the FP64 oracle. FP16 storage does
-    not meet the 1e-4 bar of the FP32 form; its measured error is recorded with the bench.
+    p (scaled as in the FP32 parity tests) <= 1e-4 against the FP64 oracle, the mixed-precision
+    bar of the FP32 form;
+  set/get round trip: p, u, v as their FP16 values; w within half an FP16 ulp of its deviation
+    from the column's base.
 """
 import numpy as np
 import pytest
@@ -89,7 +94,7 @@ def test_fp16_config1_200_steps(built, ctx):
     got, log = run_gpu(built, ctx, dom, prm, built.F16, f, 200)
     ep, eu, eps = errors(got, ref, m2)
     print(f"FP16 small 64x32x32 pipe, 200 steps: rel L2 u {eu:.3e}, p (scaled) {eps:.3e}")
-    assert eu <= 3e-3 and eps <= 3e-3, (ep, eu, eps)
+    assert eu <= 1e-4 and eps <= 1e-4, (ep, eu, eps)
     assert [r["step"] for r in log] == [50, 100, 150, 200]
 
 
@@ -101,6 +106,13 @@ def test_fp16_set_get_round_trip(built, ctx):
     got = s.get_fields()
     want = f.astype(np.float16).astype(np.float64)
     want[:, :, m2 != 0] = 0.0
-    assert np.array_equal(got, want)
+    assert np.array_equal(got[:3], want[:3])
+    # w: the base is the column's streamwise mean, the stored deviation an FP16 value
+    base = np.where(m2 == 0, f[3].mean(axis=0), 0.0).astype(np.float32)
+    dev = f[3].astype(np.float32) - base[None]
+    assert np.all(np.abs(got[3] - f[3]) <= 0.5 * f16_ulp(dev) + 1e-7)
+    assert np.all(got[3][:, m2 != 0] == 0.0)
+    # the profile itself is not rounded: the error stays far below raw FP16 storage of w
+    assert np.max(np.abs(got[3] - f[3])) < 0.01 * 0.5 * np.max(f16_ulp(f[3][:, m2 == 0]))
     assert s.info()["dtype"] == fb.F16
     s.close()
