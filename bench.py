@@ -682,7 +682,8 @@ def run_mixed(args):
         row = {}
         for name in ("f32", "f16"):
             row[name] = {"rel_l2_u": float(np.linalg.norm(f[name][1:] - ref[1:]) / np.linalg.norm(ref[1:])),
-                         "rel_l2_p": float(np.linalg.norm(f[name][0] - ref[0]) / np.linalg.norm(ref[0]))}
+                         "rel_l2_p": float(np.linalg.norm(f[name][0] - ref[0]) / np.linalg.norm(ref[0])),
+                         "rel_l2_rho": float(np.linalg.norm(f[name][0] - ref[0]) / np.linalg.norm(1.0 + ref[0]))}
         out[f"re{int(re)}"] = row
     rates = {}
     for name, dt in (("f64", fb.F64), ("f32", fb.F32), ("f16", fb.F16)):

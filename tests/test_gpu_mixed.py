@@ -45,11 +45,20 @@ def test_fp16_one_step_within_one_ulp_and_unbiased(built, ctx):
     f[1:3] = 0.03 * rng.uniform(-1, 1, f[1:3].shape)
     f[3] = -0.4 + 0.05 * rng.uniform(-1, 1, f[3].shape)
     f[:, :, m2 != 0] = 0.0
-    f = f.astype(np.float16).astype(np.float64)          # FP16-exact input
+    f = f.astype(np.float16).astype(np.float64)
     prm = dict(tblend=0.8, pin=0.002, nu=0.02, d1=2, blend=1.0, force=(0.0, 0.0, -1e-5))
-    ref, _ = O.run_core(m2, L, f.astype(np.float32), prm, 1, monitor_every=0, dtype=np.float32)
+    # the oracle steps the state the solve holds: p, u, v as given (FP16-exact), w as the
+    # column's base plus the stored FP16 deviation (one rounding at set_fields)
+    sv = fb.Solve(ctx, dom, to_params(fb, prm, 0), fb.F16)
+    sv.set_fields(f)
+    held = sv.get_fields()
+    sv.step(1)
+    sv.sync()
+    got = sv.get_fields()
+    sv.close()
+    assert np.array_equal(held[:3], f[:3])
+    ref, _ = O.run_core(m2, L, held.astype(np.float32), prm, 1, monitor_every=0, dtype=np.float32)
     ref = ref.astype(np.float64)
-    got, _ = run_gpu(fb, ctx, dom, prm, fb.F16, f, 1, monitor_every=0)
     nw = m2 == 0
     d = (got - ref)[:, :, nw]
     ulp = f16_ulp(np.maximum(np.abs(got), np.abs(ref)))[:, :, nw]
