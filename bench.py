@@ -395,36 +395,46 @@ def _member_start(fb, s, sp):
 
 
 def run_ensemble(args):
-    """Mixed-size ensemble (64 seeded pipes, L in [32,256], n in [24,96], Re in [50,3000],
-    FP32): the batched persistent launch against the same pipes stepped one at a time."""
+    """Mixed-size ensemble (64 seeded pipes, L in [32,256], n in [24,96], Re in [50,3000]):
+    the batched persistent launch (FP32 storage, or FP16 storage with --ensemble-dtype f16)
+    against the same pipes stepped one at a time by the plain FP32 method."""
     import flowcontrast_b200 as fb
     from flowcontrast_b200 import build, workloads as wl
     build.build()
     ctx = fb.Context(0)
     specs = wl.ensemble(64, steps=args.steps)
     cells = sum(sp.cells for sp in specs)
+    dt = fb.F16 if args.ensemble_dtype == "f16" else fb.F32
 
-    def fresh():
-        out = [fb.Solve(ctx, sp.domain(fb), sp.params(fb), fb.F32) for sp in specs]
+    def fresh(dtype=dt):
+        out = [fb.Solve(ctx, sp.domain(fb), sp.params(fb), dtype) for sp in specs]
         for sp, s in zip(specs, out):
             _member_start(fb, s, sp)
         for s in out:
             s.sync()
         return out
 
-    # one at a time on the plain path (device time of each member's K steps, summed)
-    solves = fresh()
-    for s in solves:
-        s.step(args.warmup)
-    plain_ms = 0.0
-    for s in solves:
-        s.sync()
-        s.step(args.steps)
-        s.sync()
-        plain_ms += s.info()["last_step_ms"]
-    plain_fields = [s.get_fields(np.float32) for s in solves]
-    for s in solves:
-        s.close()
+    def one_at_a_time(dtype):
+        """Device time of each member's K steps on the plain path, summed; final fields."""
+        solves = fresh(dtype)
+        for s in solves:
+            s.step(args.warmup)
+        ms = 0.0
+        for s in solves:
+            s.sync()
+            s.step(args.steps)
+            s.sync()
+            ms += s.info()["last_step_ms"]
+        fields = [s.get_fields(np.float32) for s in solves]
+        for s in solves:
+            s.close()
+        return ms, fields
+
+    # the plain method (FP32) one at a time, and the same storage type alone for the bitwise check
+    plain_ms, plain_fields = one_at_a_time(fb.F32)
+    alone_ms = plain_ms
+    if dt != fb.F32:
+        alone_ms, plain_fields = one_at_a_time(dt)
 
     # batched, default tiling (the shipped table): the same starts, chained steps (one
     # persistent launch per 16 steps, replayed from a CUDA graph)
@@ -487,13 +497,16 @@ def run_ensemble(args):
     line = {"metric": "aggregate MLUPS, batched ensemble (all box cells)", "value": value,
             "unit": "MLUPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": batch_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ensemble)",
+            "vs_baseline": None, "dtype": args.ensemble_dtype, "data": "synthetic (seeded ensemble)",
             "config": {"workload": "64 seeded pipes, L~U[32,256] streamwise, n~U[24,96] square "
                                    "cross-section, R=n/2-1, Re log-uniform [50,3000] (u_b 0.1), "
-                                   "tblend 0.02, d1 2, order-4 blend, FP32",
+                                   "tblend 0.02, d1 2, order-4 blend, "
+                                   + ("FP16 storage (FP32 arithmetic)" if dt == fb.F16 else "FP32")
+                                   + "; baseline: the plain FP32 method one pipe at a time",
                        "cells": cells, "members": len(specs),
                        "l2": f"inputs larger than L2: {2 * 16 * cells / 1e9:.2f} GB of state"},
             "plain_one_at_a_time_mlups": plain, "speedup_vs_plain": value / plain,
+            "same_storage_one_at_a_time_mlups": cells * args.steps / (alone_ms * 1e-3) / 1e6,
             "default_tiling_mlups": cells * args.steps / (default_ms * 1e-3) / 1e6,
             "autotune": {"seconds": t_tune, "classes": len(table), "trial_steps": 20},
             "batch_equals_plain_bitwise": bool(same),
@@ -721,6 +734,8 @@ def main():
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--workload", default="plain", choices=["plain", "ensemble", "served", "mixed"])
     ap.add_argument("--requests", type=int, default=1000, help="served workload: request count")
+    ap.add_argument("--ensemble-dtype", default="f32", choices=["f32", "f16"],
+                    help="ensemble workload: storage type of the batched members")
     ap.add_argument("--served-dtype", default="mixed", choices=["mixed", "f32"],
                     help="served workload: storage types of the requests (FP32/FP16 50/50, or FP32)")
     ap.add_argument("--tuning-out", default=None, help="ensemble workload: write the tuned tiling table here")
