@@ -514,7 +514,7 @@ def run_ensemble(args):
                          "frac": achieved / peak,
                          "traffic": None,
                          "peak_source": f"{peak_kind} hbm_gbs",
-                         "kernel": "fslbm_step2_batch_kernel<2,32,scalar,float> (chained steps)"},
+                         "kernel": "fslbm_step2_batch_kernel<2,32,packed,float> (chained steps)"},
             "e2e": {"value": cells * args.steps / e2e_s / 1e6, "unit": "MLUPS",
                     "h2d_bytes_per_step": 16.0 * cells / args.steps,
                     "d2h_bytes_per_step": 16.0 * cells / args.steps},

@@ -1530,10 +1530,10 @@ extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, in
   default_tiling(b);
   if (const char* ec = std::getenv("FSLBM_BATCH_CHUNK"))
     for (int& c : b->m_chunk) c = std::max(8, std::atoi(ec));
-  // scalar pair arithmetic: with both warp shapes in one kernel the packed FP32x2 variant spills
-  // registers (FSLBM_BATCH_PACKED=1 selects it, for comparisons)
+  // packed FP32x2 pair arithmetic, as the single-pipe kernel (FSLBM_BATCH_PACKED=0 selects the
+  // scalar form, for comparisons; both give the same bits)
   const char* ebp = std::getenv("FSLBM_BATCH_PACKED");
-  b->packed = (ebp && std::atoi(ebp) == 1) ? 1 : 0;
+  b->packed = (ebp && std::atoi(ebp) == 0) ? 0 : 1;
   cudaError_t e = cudaSetDevice(ctx->device);
   if (!e && fast) e = batch_prepare(solves[0]->dtype);
   if (!e && fast) e = ctx_alloc(ctx, &b->d_members, batch_member_bytes() * n);

@@ -387,13 +387,9 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
     if (s_done < mb.stop_at) {
       const int cur = mb.cur0 ^ (step & 1);
       const int ntiles = mb.g.ntiles;
-      // the warp shape is a compile-time choice (a runtime one raises register pressure)
-      const bool ok = mb.w16x4 ? step2_march<D1, TY, PK, TE, true>(&mb.map_p[cur], &mb.map_u[cur], s_g,
-                                                                   s_k, it.y % ntiles, it.y / ntiles,
-                                                                   smem, !first)
-                               : step2_march<D1, TY, PK, TE, false>(&mb.map_p[cur], &mb.map_u[cur], s_g,
-                                                                    s_k, it.y % ntiles, it.y / ntiles,
-                                                                    smem, !first);
+      const bool ok = step2_march<D1, TY, PK, TE>(&mb.map_p[cur], &mb.map_u[cur], s_g, s_k,
+                                                  it.y % ntiles, it.y / ntiles, smem, !first,
+                                                  mb.w16x4 != 0);
       if (!ok) return;
       first = false;
     }

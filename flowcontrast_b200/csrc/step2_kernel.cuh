@@ -187,10 +187,14 @@ __device__ __forceinline__ float2 qof(float2 P, float2 U, float2 V, float2 W) {
 // Freed window slots are refilled by the last warp to release them (no warp waits for a free
 // slot); measured +2 % on the single pipe and +1.7 % on the batched ensemble against thread 0
 // waiting on per-slot "empty" mbarriers and refilling.
-template <int D1, int TY, bool PK, class TE, bool W16X4 = false>
+// The warp shape (w16x4, below) is a runtime argument: it only places each thread in the tile, and
+// a kernel that inlines one march for both shapes (the batched kernel, whose members choose
+// their shape) keeps one copy of the march instead of two, which ended its register spills.
+template <int D1, int TY, bool PK, class TE>
 __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUtensorMap* tmap_uvw,
                                             const Step2Geom& g, const StepConst<float>& k,
-                                            int tile, int chunk, unsigned char* smem, bool reinit) {
+                                            int tile, int chunk, unsigned char* smem, bool reinit,
+                                            bool w16x4 = false) {
   using Tl = Step2Tile<D1, TY, TE>;
   using F = Pair<PK>;
   static_assert(D1 == 2, "the march prologue below is written for d1 = 2 (R = 4)");
@@ -203,15 +207,15 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
   unsigned* released = reinterpret_cast<unsigned*>(full + S);
 
   // Warp shape. Default: 32 columns x 2 rows (each half-warp reads one contiguous row).
-  // W16X4: 16 columns (8 pairs) x 4 rows, so warps over wall skip at a finer grain, which pays
+  // w16x4: 16 columns (8 pairs) x 4 rows, so warps over wall skip at a finer grain, which pays
   // for small cross-sections (measured +6 % on the mixed-size ensemble, -2 % on the 128 x 128
   // pipe). There lanes 0-15 take rows 0 and 2 of the warp and lanes 16-31 rows 1 and 3: with the
   // 160-byte FP32 row stride each half-warp's 64-bit shared loads fall on distinct banks (FP16
   // rows of 96 bytes are conflict-free in any order). The map changes no thread's arithmetic.
   static_assert(Tl::TX == 32 && TY % 4 == 0, "warp shapes within a 32-wide tile");
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int tp = W16X4 ? (warp & 1) * 8 + (lane & 7) : tid % (Tl::TX / 2);
-  const int ty = W16X4 ? (warp >> 1) * 4 + ((lane >> 3) & 1) * 2 + (lane >> 4) : tid / (Tl::TX / 2);
+  const int tp = w16x4 ? (warp & 1) * 8 + (lane & 7) : tid % (Tl::TX / 2);
+  const int ty = w16x4 ? (warp >> 1) * 4 + ((lane >> 3) & 1) * 2 + (lane >> 4) : tid / (Tl::TX / 2);
 
   // ---- work: one (tile, chunk); odd chunks march towards -z
   const int zb = int((long long)g.L * chunk / g.nchunks);
