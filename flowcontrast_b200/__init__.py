@@ -494,8 +494,9 @@ class Batch:
         """Member `member` stops stepping once its step count reaches stop_step (-1: never)."""
         _check(lib().fslbm_batch_set_stop(self.handle, int(member), int(stop_step)))
 
-    def set_tiling(self, member, chunk, warp16x4=True):
-        _check(lib().fslbm_batch_set_tiling(self.handle, int(member), int(chunk), int(bool(warp16x4))))
+    def set_tiling(self, member, chunk, warp_shape=1):
+        """warp_shape: 0 = 32 x 2 cells, 1 = 16 x 4, 2 = 8 x 8."""
+        _check(lib().fslbm_batch_set_tiling(self.handle, int(member), int(chunk), int(warp_shape)))
 
     def load_tiling(self, path):
         _check(lib().fslbm_batch_load_tiling(self.handle, os.fsencode(path)))

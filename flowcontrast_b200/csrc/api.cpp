@@ -205,7 +205,7 @@ struct fslbm_solve {
   // FP32 column-pair kernel (even d1): tile height, persistent grid, two maps per buffer
   bool use2 = false;
   int ty2 = 32, grid2 = 0, packed2 = 1;
-  std::vector<int> tile_warps[2];  // per column-pair tile: warps holding fluid, [0] 32 x 2, [1] 16 x 4
+  std::vector<int> tile_warps[3];  // per column-pair tile: warps holding fluid, [shape] 32 x 2, 16 x 4, 8 x 8
   CUtensorMap maps2p[2], maps2u[2];
   DevCounters* d_counters = nullptr;
   fslbm_monitor* d_log = nullptr;
@@ -268,44 +268,57 @@ static int validate_params(const fslbm_params* p, int dtype) {
   return FSLBM_OK;
 }
 
+// Tensor maps of the column-pair kernel with tile height ty over the solve's two state buffers:
+// the p box (one-cell halo) and the u,v,w box (the corrector's halo).
+static int encode_pair_maps(const fslbm_solve* s, int ty, CUtensorMap mp[2], CUtensorMap mu[2]) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return fslbm_set_error(FSLBM_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+  const CUtensorMapDataType dt = s->dtype == FSLBM_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                       : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  int sw2, ph, uh, hx2, hy2;
+  if (!step2_box(s->dtype, s->prm.d1, ty, &sw2, &ph, &uh, &hx2, &hy2))
+    return fslbm_set_error(FSLBM_ERR_ARG, "no column-pair kernel for d1 %d, tile height %d", s->prm.d1, ty);
+  cuuint64_t dims[4] = {cuuint64_t(s->lxp), cuuint64_t(s->ly), cuuint64_t(s->L), 4};
+  cuuint64_t strides[3] = {cuuint64_t(s->lxp) * s->es, cuuint64_t(s->lxp) * s->ly * s->es,
+                           cuuint64_t(field_stride(s)) * s->es};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  cuuint32_t boxp[4] = {cuuint32_t(sw2), cuuint32_t(ph), 1, 1};
+  cuuint32_t boxu[4] = {cuuint32_t(sw2), cuuint32_t(uh), 1, 3};
+  for (int b = 0; b < 2; ++b) {
+    CUresult r = enc(&mp[b], dt, 4, s->state[b], dims, strides, boxp, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r == CUDA_SUCCESS)
+      r = enc(&mu[b], dt, 4, s->state[b], dims, strides, boxu, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+      return fslbm_set_error(FSLBM_ERR_CUDA, "cuTensorMapEncodeTiled (pair kernel) failed (%d)", int(r));
+  }
+  return FSLBM_OK;
+}
+
 static int build_tensor_maps(fslbm_solve* s) {
+  if (s->use2) return encode_pair_maps(s, s->ty2, s->maps2p, s->maps2u);
   EncodeTiledFn enc = encode_fn();
   if (!enc) return fslbm_set_error(FSLBM_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
   const CUtensorMapDataType dt = s->dtype == FSLBM_F64   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
                                  : s->dtype == FSLBM_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
                                                          : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  int sw, sh, hx, hy;
+  if (!step_box(s->dtype, s->prm.d1, s->K, &sw, &sh, &hx, &hy))
+    return fslbm_set_error(FSLBM_ERR_ARG, "no step kernel for dtype %d d1 %d", s->dtype, s->prm.d1);
+  cuuint64_t dims[4] = {cuuint64_t(s->lxp), cuuint64_t(s->ly), cuuint64_t(s->L), 4};
+  cuuint64_t strides[3] = {cuuint64_t(s->lxp) * s->es, cuuint64_t(s->lxp) * s->ly * s->es,
+                           cuuint64_t(field_stride(s)) * s->es};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  cuuint32_t box[4] = {cuuint32_t(sw), cuuint32_t(sh), 1, 4};
   for (int b = 0; b < 2; ++b) {
-    cuuint64_t dims[4] = {cuuint64_t(s->lxp), cuuint64_t(s->ly), cuuint64_t(s->L), 4};
-    cuuint64_t strides[3] = {cuuint64_t(s->lxp) * s->es, cuuint64_t(s->lxp) * s->ly * s->es,
-                             cuuint64_t(field_stride(s)) * s->es};
-    cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r;
-    if (!s->use2) {
-      int sw, sh, hx, hy;
-      if (!step_box(s->dtype, s->prm.d1, s->K, &sw, &sh, &hx, &hy))
-        return fslbm_set_error(FSLBM_ERR_ARG, "no step kernel for dtype %d d1 %d", s->dtype, s->prm.d1);
-      cuuint32_t box[4] = {cuuint32_t(sw), cuuint32_t(sh), 1, 4};
-      r = enc(&s->maps[b], dt, 4, s->state[b], dims, strides, box, estr,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r != CUDA_SUCCESS)
-        return fslbm_set_error(FSLBM_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
-    } else {
-      int sw2, ph, uh, hx2, hy2;
-      if (!step2_box(s->dtype, s->prm.d1, s->ty2, &sw2, &ph, &uh, &hx2, &hy2))
-        return fslbm_set_error(FSLBM_ERR_ARG, "no column-pair kernel for d1 %d", s->prm.d1);
-      cuuint32_t boxp[4] = {cuuint32_t(sw2), cuuint32_t(ph), 1, 1};
-      cuuint32_t boxu[4] = {cuuint32_t(sw2), cuuint32_t(uh), 1, 3};
-      r = enc(&s->maps2p[b], dt, 4, s->state[b], dims, strides, boxp, estr,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r == CUDA_SUCCESS)
-        r = enc(&s->maps2u[b], dt, 4, s->state[b], dims, strides, boxu, estr,
-                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r != CUDA_SUCCESS)
-        return fslbm_set_error(FSLBM_ERR_CUDA, "cuTensorMapEncodeTiled (pair kernel) failed (%d)", int(r));
-    }
+    const CUresult r = enc(&s->maps[b], dt, 4, s->state[b], dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+      return fslbm_set_error(FSLBM_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
   }
   return FSLBM_OK;
 }
@@ -325,6 +338,27 @@ static std::vector<int2> fluid_tiles(const fslbm_solve* s, int th) {
   return tiles;
 }
 
+// Warps of each column-pair tile (32 x ty cells) that hold fluid, for the three warp shapes:
+// warps[0] 32 x 2 cells, warps[1] 16 x 4 cells, warps[2] 8 x 8 cells (the kernel's lane maps).
+static void tile_warp_counts(const fslbm_solve* s, const std::vector<int2>& tiles, int ty,
+                             std::vector<int> (&warps)[3]) {
+  static const int kWx[3] = {32, 16, 8}, kWy[3] = {2, 4, 8};
+  for (const int2 org : tiles)
+    for (int shape = 0; shape < 3; ++shape) {
+      const int wx = kWx[shape], wy = kWy[shape], across = 32 / wx;
+      int n = 0;
+      for (int w = 0; w < ty / 2; ++w) {
+        const int x0 = org.x + wx * (w % across), y0 = org.y + wy * (w / across);
+        bool any = false;
+        for (int y = y0; y < std::min(y0 + wy, s->ly) && !any; ++y)
+          for (int x = x0; x < std::min(x0 + wx, s->lxp) && !any; ++x)
+            any = s->mask[size_t(y) * s->lxp + x] == 0;
+        n += any;
+      }
+      warps[shape].push_back(n);
+    }
+}
+
 static void choose_chunks(fslbm_solve* s);
 
 // Selects the step kernel for the current dtype and d1, uploads its tile list, builds its
@@ -342,23 +376,8 @@ static int configure_kernel(fslbm_solve* s) {
   const char* ep = std::getenv("FSLBM_PACKED");
   s->packed2 = (ep && std::atoi(ep) == 0) ? 0 : 1;
   const std::vector<int2> tiles = fluid_tiles(s, s->use2 ? s->ty2 : kTY);
-  s->tile_warps[0].clear();
-  s->tile_warps[1].clear();
-  if (s->use2)
-    for (const int2 org : tiles)
-      for (int shape = 0; shape < 2; ++shape) {
-        const int wx = shape ? 16 : 32, wy = shape ? 4 : 2;
-        int warps = 0;
-        for (int w = 0; w < s->ty2 / 2; ++w) {
-          const int x0 = org.x + (shape ? 16 * (w & 1) : 0), y0 = org.y + (shape ? 4 * (w >> 1) : 2 * w);
-          bool any = false;
-          for (int y = y0; y < std::min(y0 + wy, s->ly) && !any; ++y)
-            for (int x = x0; x < std::min(x0 + wx, s->lxp) && !any; ++x)
-              any = s->mask[size_t(y) * s->lxp + x] == 0;
-          warps += any;
-        }
-        s->tile_warps[shape].push_back(warps);
-      }
+  for (auto& v : s->tile_warps) v.clear();
+  if (s->use2) tile_warp_counts(s, tiles, s->ty2, s->tile_warps);
   if (s->d_tiles) {
     ctx_free(s->ctx, s->d_tiles);
     s->bytes_device -= int64_t(s->ntiles) * sizeof(int2);
@@ -372,6 +391,8 @@ static int configure_kernel(fslbm_solve* s) {
   if (s->use2) {
     CUDA_TRY(step2_prepare(s->dtype, s->prm.d1, s->ty2));
     // tiles x streamwise chunks, at most one CTA per SM slot and chunks of at least 2R planes
+    // (chunk counts weighted by each tile's fluid warps measured no faster: a tile with wall in
+    // it is not proportionally faster per plane)
     const int slots = s->ctx->sm_count * step2_occupancy(s->prm.d1, s->ty2);
     int nch = std::max(1, slots / s->ntiles);
     nch = std::min(nch, std::max(1, s->L / (4 * s->prm.d1)));
@@ -1277,9 +1298,21 @@ struct fslbm_batch {
   std::vector<int2> h_items;
   std::vector<int2> item_shape;    // per member: (tiles, chunks) the item table was built for
   int nitems = 0, grid = 0, packed = 1;
-  // per member tiling: streamwise planes per work item and warp shape (16 x 4 or 32 x 2),
-  // from the tuning table by size class, else 128 (FSLBM_BATCH_CHUNK) and 16 x 4
-  std::vector<int> m_chunk, m_w4;
+  // the batch's own column-pair tiling of every member (32 x ty tiles, one height for the whole
+  // batch): tile list, fluid warps per tile for the two warp shapes, tensor maps of both buffers.
+  // 32 x 16 tiles, two 256-thread CTAs per SM: on the 64-pipe ensemble (cross-sections 24..96)
+  // +1.0 % against 32 x 32 tiles; the members' own single-pipe tiling is not affected
+  int ty = 16;
+  struct Tiling {
+    int ntiles = 0;
+    int2* d_tiles = nullptr;
+    std::vector<int> warps[3];
+    CUtensorMap mp[2], mu[2];
+  };
+  std::vector<Tiling> mt;
+  // per member tiling: streamwise planes per work item and warp shape (0: 32 x 2, 1: 16 x 4,
+  // 2: 8 x 8), from the tuning table by size class, else 128 (FSLBM_BATCH_CHUNK) and 16 x 4
+  std::vector<int> m_chunk, m_shape;
   int shrink = 1;                  // chunk divisor for batches with fewer than 2 items per SM
   cudaGraphExec_t exec2 = nullptr;  // one chained launch of `chain` steps
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1290,6 +1323,7 @@ static void free_batch(fslbm_batch* b) {
   if (!b) return;
   cudaSetDevice(b->ctx->device);
   if (b->exec2) cudaGraphExecDestroy(b->exec2);
+  for (auto& t : b->mt) ctx_free(b->ctx, t.d_tiles);
   ctx_free(b->ctx, b->d_members);
   ctx_free(b->ctx, b->d_mons);
   ctx_free(b->ctx, b->d_items);
@@ -1305,8 +1339,14 @@ static void free_batch(fslbm_batch* b) {
 // Work of one (tile, chunk) item of the column-pair kernel, for ordering the items: planes
 // marched (the chunk plus the 2R pipeline planes) times the tile's warps that compute plus two
 // for the pipeline's fixed cost.
-static int64_t item_cost(const fslbm_solve* s, int tile, int nout, int w16x4) {
-  return int64_t(nout + 4 * s->prm.d1) * (s->tile_warps[w16x4 ? 1 : 0][tile] + 2);
+static int64_t item_cost(const fslbm_solve* s, const std::vector<int> (&warps)[3], int tile, int nout,
+                         int shape) {
+  return int64_t(nout + 4 * s->prm.d1) * (warps[shape][tile] + 2);
+}
+
+// Resident CTAs of the batched kernel: one per SM for 32 x 32 tiles, two for 32 x 16 tiles.
+static int batch_slots(const fslbm_batch* b) {
+  return b->ctx->sm_count * step2_occupancy(2, b->ty);
 }
 
 // Streamwise chunks of a member: about `chunk` planes each, at least 4*d1 planes.
@@ -1329,14 +1369,14 @@ static int batch_upload(fslbm_batch* b) {
   // (stride, corrector order or storage type changed) is refused
   for (int i = 0; i < n; ++i) {
     const fslbm_solve* s = b->members[i];
-    if (!(s->use2 && s->ty2 == 32 && s->prm.d1 == 2 && s->dtype == b->members[0]->dtype && s->nghost == 0))
+    if (!(s->use2 && s->prm.d1 == 2 && s->dtype == b->members[0]->dtype && s->nghost == 0))
       return fslbm_set_error(FSLBM_ERR_STATE, "batch_step: member %d was reconfigured and no longer "
                              "fits the batched kernel; create a new batch", i);
   }
   auto eff_chunk = [&](int i) { return std::max(4 * b->members[i]->prm.d1, b->m_chunk[i] / b->shrink); };
   if (!b->h_items.empty() && b->item_shape.size() == size_t(n))
     for (int i = 0; i < n; ++i)
-      if (b->item_shape[i].x != b->members[i]->ntiles ||
+      if (b->item_shape[i].x != b->mt[i].ntiles ||
           b->item_shape[i].y != member_chunks(b->members[i], eff_chunk(i))) {
         b->h_items.clear();
         break;
@@ -1348,41 +1388,42 @@ static int batch_upload(fslbm_batch* b) {
     // shorter chunks while there are fewer than two items per SM (few or small members)
     auto count = [&]() {
       int64_t c = 0;
-      for (int i = 0; i < n; ++i) c += int64_t(b->members[i]->ntiles) * member_chunks(b->members[i], eff_chunk(i));
+      for (int i = 0; i < n; ++i) c += int64_t(b->mt[i].ntiles) * member_chunks(b->members[i], eff_chunk(i));
       return c;
     };
     b->shrink = 1;
-    while (b->shrink < 64 && count() < 2 * b->ctx->sm_count) b->shrink *= 2;
+    while (b->shrink < 64 && count() < 2 * batch_slots(b)) b->shrink *= 2;
   }
   for (int i = 0; i < n; ++i) {
     fslbm_solve* s = b->members[i];
+    const fslbm_batch::Tiling& tl = b->mt[i];
     StepLaunch a{};
     a.dtype = s->dtype; a.d1 = s->prm.d1;
-    a.lxp = s->lxp; a.ly = s->ly; a.L = s->L; a.ntiles = s->ntiles;
-    a.tiles = s->d_tiles; a.mask = s->d_mask; a.colcoef = s->d_colcoef;
+    a.lxp = s->lxp; a.ly = s->ly; a.L = s->L; a.ntiles = tl.ntiles;
+    a.tiles = tl.d_tiles; a.mask = s->d_mask; a.colcoef = s->d_colcoef;
     a.err = b->d_tickets + 2;        // one flag for the whole batch
     a.wb = s->d_wbase; a.wgt = s->d_wgt;
     fill_constants(s, a);
     const int nch = member_chunks(s, eff_chunk(i));
     const long long stop_at = b->stop[i] >= 0 ? (long long)b->stop[i] : LLONG_MAX;
-    CUDA_TRY(fill_batch_member(b->h_members.data() + mbytes * i, s->maps2p, s->maps2u, a,
+    CUDA_TRY(fill_batch_member(b->h_members.data() + mbytes * i, tl.mp, tl.mu, a,
                                s->state[0], s->state[1], s->d_gauge, &s->d_counters->steps,
-                               stop_at, s->prm.monitor_every, s->cur, nch, b->m_w4[i]));
+                               stop_at, s->prm.monitor_every, s->cur, nch, b->m_shape[i]));
     if (build_items) {
       if (i == 0) b->item_shape.assign(n, make_int2(0, 0));
-      b->item_shape[i] = make_int2(s->ntiles, nch);
+      b->item_shape[i] = make_int2(tl.ntiles, nch);
     }
     if (build_items)
       for (int c = 0; c < nch; ++c) {
         const int nout = int((long long)s->L * (c + 1) / nch - (long long)s->L * c / nch);
-        for (int t = 0; t < s->ntiles; ++t)
-          items.push_back({item_cost(s, t, nout, b->m_w4[i]), make_int2(i, c * s->ntiles + t)});
+        for (int t = 0; t < tl.ntiles; ++t)
+          items.push_back({item_cost(s, tl.warps, t, nout, b->m_shape[i]), make_int2(i, c * tl.ntiles + t)});
         // the chunk's tiles are ordered by the chunk's longest tile, so neighbouring tiles are
         // claimed one after another and read their shared halo planes while they are in L2
         int64_t longest = 0;
-        for (size_t k = items.size() - size_t(s->ntiles); k < items.size(); ++k)
+        for (size_t k = items.size() - size_t(tl.ntiles); k < items.size(); ++k)
           longest = std::max(longest, items[k].cost);
-        for (size_t k = items.size() - size_t(s->ntiles); k < items.size(); ++k) items[k].cost = longest;
+        for (size_t k = items.size() - size_t(tl.ntiles); k < items.size(); ++k) items[k].cost = longest;
       }
     BatchMon& m = b->h_mons[i];
     std::memset(&m, 0, sizeof m);
@@ -1402,7 +1443,7 @@ static int batch_upload(fslbm_batch* b) {
     b->h_items.resize(items.size());
     for (size_t k = 0; k < items.size(); ++k) b->h_items[k] = items[k].it;
     b->nitems = int(items.size());
-    b->grid = std::max(1, std::min(b->nitems, b->ctx->sm_count));
+    b->grid = std::max(1, std::min(b->nitems, batch_slots(b)));
     ctx_free(b->ctx, b->d_items);
     b->d_items = nullptr;
     CUDA_TRY(ctx_alloc(b->ctx, reinterpret_cast<void**>(&b->d_items), b->h_items.size() * sizeof(int2)));
@@ -1422,7 +1463,7 @@ static int batch_upload(fslbm_batch* b) {
 
 // One chained launch of `nsteps` steps for every member (each starting at its buffer cur0).
 static cudaError_t batch_enqueue(fslbm_batch* b, int nsteps, cudaStream_t st) {
-  return launch_batch_steps(b->members[0]->dtype, b->d_members, b->d_mons, b->d_items, b->nitems,
+  return launch_batch_steps(b->members[0]->dtype, b->ty, b->d_members, b->d_mons, b->d_items, b->nitems,
                             nsteps, b->grid, b->packed, b->d_sync, int(b->members.size()),
                             b->d_tickets + 2, st);
 }
@@ -1440,7 +1481,7 @@ static std::string class_key(const fslbm_solve* s) {
   return buf;
 }
 
-struct Tiling { int chunk = 128, w16x4 = 1; double ms = 0; };
+struct Tiling { int chunk = 128, shape = 1; double ms = 0; };
 using TilingTable = std::map<std::string, Tiling>;
 
 static bool write_tiling(const char* path, const TilingTable& t) {
@@ -1449,15 +1490,16 @@ static bool write_tiling(const char* path, const TilingTable& t) {
   std::fprintf(f, "{\n  \"format\": \"fslbm batch tiling 1\",\n  \"classes\": {");
   bool first = true;
   for (const auto& kv : t) {
-    std::fprintf(f, "%s\n    \"%s\": {\"chunk\": %d, \"warp16x4\": %d, \"trial_ms\": %.4f}",
-                 first ? "" : ",", kv.first.c_str(), kv.second.chunk, kv.second.w16x4, kv.second.ms);
+    std::fprintf(f, "%s\n    \"%s\": {\"chunk\": %d, \"warp_shape\": %d, \"trial_ms\": %.4f}",
+                 first ? "" : ",", kv.first.c_str(), kv.second.chunk, kv.second.shape, kv.second.ms);
     first = false;
   }
   std::fprintf(f, "\n  }\n}\n");
   return std::fclose(f) == 0;
 }
 
-// Reads the table written by write_tiling: every `"<key>": {"chunk": N, "warp16x4": M` entry.
+// Reads the table written by write_tiling: every `"<key>": {"chunk": N, "warp_shape": M` entry
+// (M = 0, 1, 2; tables of the earlier form name it "warp16x4", 0 or 1, with the same meaning).
 static bool read_tiling(const char* path, TilingTable& t) {
   FILE* f = std::fopen(path, "rb");
   if (!f) return false;
@@ -1472,8 +1514,9 @@ static bool read_tiling(const char* path, TilingTable& t) {
     const size_t q0 = q1 == std::string::npos ? q1 : s.rfind('"', q1 - 1);
     Tiling v;
     if (q0 != std::string::npos &&
-        std::sscanf(s.c_str() + pos, "{\"chunk\": %d, \"warp16x4\": %d", &v.chunk, &v.w16x4) == 2 &&
-        v.chunk >= 4)
+        (std::sscanf(s.c_str() + pos, "{\"chunk\": %d, \"warp_shape\": %d", &v.chunk, &v.shape) == 2 ||
+         std::sscanf(s.c_str() + pos, "{\"chunk\": %d, \"warp16x4\": %d", &v.chunk, &v.shape) == 2) &&
+        v.chunk >= 4 && v.shape >= 0 && v.shape <= 2)
       t[s.substr(q0 + 1, q1 - q0 - 1)] = v;
     pos += 9;
   }
@@ -1485,7 +1528,7 @@ static void apply_tiling(fslbm_batch* b, const TilingTable& t) {
     auto it = t.find(class_key(b->members[i]));
     if (it == t.end()) continue;
     b->m_chunk[i] = it->second.chunk;
-    b->m_w4[i] = it->second.w16x4 ? 1 : 0;
+    b->m_shape[i] = it->second.shape;
   }
   b->h_items.clear();              // rebuild the work items
 }
@@ -1522,8 +1565,8 @@ extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, in
     b->members.push_back(solves[i]);
     b->stop.push_back(-1);
     b->m_chunk.push_back(128);
-    b->m_w4.push_back(1);
-    fast = fast && solves[i]->use2 && solves[i]->ty2 == 32 && solves[i]->prm.d1 == 2 &&
+    b->m_shape.push_back(1);
+    fast = fast && solves[i]->use2 && solves[i]->prm.d1 == 2 &&
            solves[i]->dtype == solves[0]->dtype && solves[i]->nghost == 0;
   }
   b->fast = fast;
@@ -1535,7 +1578,27 @@ extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, in
   const char* ebp = std::getenv("FSLBM_BATCH_PACKED");
   b->packed = (ebp && std::atoi(ebp) == 0) ? 0 : 1;
   cudaError_t e = cudaSetDevice(ctx->device);
-  if (!e && fast) e = batch_prepare(solves[0]->dtype);
+  // tile height of the batch's tiles (FSLBM_BATCH_TILE_Y=16|32 overrides the default)
+  if (const char* ety = std::getenv("FSLBM_BATCH_TILE_Y")) b->ty = std::atoi(ety) == 16 ? 16 : 32;
+  if (!e && fast) e = batch_prepare(solves[0]->dtype, b->ty);
+  if (!e && fast) {
+    b->mt.resize(n);
+    for (int i = 0; i < n && !e; ++i) {
+      fslbm_solve* s = solves[i];
+      fslbm_batch::Tiling& tl = b->mt[i];
+      const std::vector<int2> tiles = fluid_tiles(s, b->ty);
+      tl.ntiles = int(tiles.size());
+      tile_warp_counts(s, tiles, b->ty, tl.warps);
+      const int rc = encode_pair_maps(s, b->ty, tl.mp, tl.mu);
+      if (rc != FSLBM_OK) {
+        free_batch(b);
+        return rc;
+      }
+      e = ctx_alloc(ctx, reinterpret_cast<void**>(&tl.d_tiles), std::max<size_t>(1, tiles.size()) * sizeof(int2));
+      if (!e) e = cudaMemcpyAsync(tl.d_tiles, tiles.data(), tiles.size() * sizeof(int2),
+                                  cudaMemcpyHostToDevice, ctx->stream);
+    }
+  }
   if (!e && fast) e = ctx_alloc(ctx, &b->d_members, batch_member_bytes() * n);
   if (!e && fast) e = ctx_alloc(ctx, reinterpret_cast<void**>(&b->d_mons), sizeof(BatchMon) * n);
   if (!e && fast) e = ctx_alloc(ctx, reinterpret_cast<void**>(&b->d_tickets), 4 * sizeof(unsigned));
@@ -1651,11 +1714,11 @@ extern "C" int fslbm_batch_elapsed(fslbm_batch* b, double* ms) {
   return FSLBM_OK;
 }
 
-extern "C" int fslbm_batch_set_tiling(fslbm_batch* b, int member, int chunk, int warp16x4) {
-  if (!b || member < 0 || member >= int(b->members.size()) || chunk < 1)
-    return fslbm_set_error(FSLBM_ERR_ARG, "batch_set_tiling: bad batch, member or chunk");
+extern "C" int fslbm_batch_set_tiling(fslbm_batch* b, int member, int chunk, int warp_shape) {
+  if (!b || member < 0 || member >= int(b->members.size()) || chunk < 1 || warp_shape < 0 || warp_shape > 2)
+    return fslbm_set_error(FSLBM_ERR_ARG, "batch_set_tiling: bad batch, member, chunk or warp shape");
   b->m_chunk[member] = chunk;
-  b->m_w4[member] = warp16x4 ? 1 : 0;
+  b->m_shape[member] = warp_shape;
   b->h_items.clear();
   return FSLBM_OK;
 }
@@ -1669,8 +1732,8 @@ extern "C" int fslbm_batch_load_tiling(fslbm_batch* b, const char* path) {
 }
 
 // Times candidate tilings on the batch itself: first one tiling for all members (chunks 64, 128,
-// 256 planes, both warp shapes), then per size class, largest first, the neighbouring chunks and
-// the other warp shape while the other classes keep theirs; a change is kept only when it is at
+// 256 planes, the three warp shapes), then per size class, largest first, the neighbouring chunks
+// and the other warp shapes while the other classes keep theirs; a change is kept only when it is at
 // least 0.3 % faster (each timing is the better of two trials). The members' fields, step
 // counts, monitor logs and gauges are restored afterwards.
 extern "C" int fslbm_batch_autotune(fslbm_batch* b, int trial_steps, const char* path) {
@@ -1724,21 +1787,23 @@ extern "C" int fslbm_batch_autotune(fslbm_batch* b, int trial_steps, const char*
     return FSLBM_OK;
   };
   auto set = [&](const std::vector<int>& mem, int c, int w) {
-    for (int i : mem) { b->m_chunk[i] = c; b->m_w4[i] = w; }
+    for (int i : mem) { b->m_chunk[i] = c; b->m_shape[i] = w; }
     b->h_items.clear();
   };
   std::vector<int> all(n);
   for (int i = 0; i < n; ++i) all[i] = i;
   Tiling glob;
   glob.ms = 1e30;
-  for (int w = 1; w >= 0 && !rc; --w)
+  for (int w : {1, 2, 0}) {
+    if (rc) break;
     for (int c : {64, 128, 256}) {
       set(all, c, w);
       double ms = 0;
       if ((rc = trial(&ms))) break;
-      if (ms < glob.ms) { glob.ms = ms; glob.chunk = c; glob.w16x4 = w; }
+      if (ms < glob.ms) { glob.ms = ms; glob.chunk = c; glob.shape = w; }
     }
-  set(all, glob.chunk, glob.w16x4);
+  }
+  set(all, glob.chunk, glob.shape);
   double cur_ms = glob.ms;
   TilingTable table;
   for (size_t oi = 0; oi < order.size() && !rc; ++oi) {
@@ -1747,16 +1812,16 @@ extern "C" int fslbm_batch_autotune(fslbm_batch* b, int trial_steps, const char*
     for (int i : mem) maxL = std::max(maxL, b->members[i]->L);
     Tiling best = glob;
     best.ms = cur_ms;
-    const std::pair<int, int> cands[] = {{glob.chunk / 2, glob.w16x4}, {glob.chunk * 2, glob.w16x4},
-                                         {glob.chunk, 1 - glob.w16x4}};
+    const std::pair<int, int> cands[] = {{glob.chunk / 2, glob.shape}, {glob.chunk * 2, glob.shape},
+                                         {glob.chunk, (glob.shape + 1) % 3}, {glob.chunk, (glob.shape + 2) % 3}};
     for (const auto& cw : cands) {
       if (cw.first < 16 || (cw.first / 2 >= maxL && cw.first > glob.chunk)) continue;
       set(mem, cw.first, cw.second);
       double ms = 0;
       if ((rc = trial(&ms))) break;
-      if (ms < best.ms * 0.997) { best.ms = ms; best.chunk = cw.first; best.w16x4 = cw.second; }
+      if (ms < best.ms * 0.997) { best.ms = ms; best.chunk = cw.first; best.shape = cw.second; }
     }
-    set(mem, best.chunk, best.w16x4);
+    set(mem, best.chunk, best.shape);
     cur_ms = best.ms;
     table[order[oi].second] = best;
   }

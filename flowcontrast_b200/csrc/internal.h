@@ -93,7 +93,7 @@ cudaError_t launch_monitor(const MonitorLaunch& a, cudaStream_t st);
 cudaError_t launch_wait_selftest(const unsigned* counter, unsigned long long limit_ns, unsigned* err,
                                  cudaStream_t st);
 
-// ---- batched ensemble (FP32 column-pair kernel, d1 = 2, tile height 32)
+// ---- batched ensemble (column-pair kernel, d1 = 2, tile height 16 or 32 for the whole batch)
 struct BatchMon {
   MonitorLaunch mon;           // state is chosen per launch from `state`
   const void* state[2];
@@ -101,20 +101,20 @@ struct BatchMon {
   int monitor_every;
   int cur0;
 };
-cudaError_t batch_prepare(int dtype);
+cudaError_t batch_prepare(int dtype, int ty);
 size_t batch_member_bytes();
 // Writes one member descriptor (layout private to the kernels) into host memory at dst.
 cudaError_t fill_batch_member(void* dst, const CUtensorMap* map_p, const CUtensorMap* map_u,
                               const StepLaunch& a, void* state0, void* state1,
                               const double* gauge_slot, const long long* steps, long long stop_at,
-                              int monitor_every, int cur0, int nchunks, int w16x4);
+                              int monitor_every, int cur0, int nchunks, int shape);
 // Advances every member `nsteps` steps (fewer for members that reach their stop) in one
 // persistent launch, preceded by a reset of the launch's counters. items: nitems (member, item
 // of the member) pairs, longest first; mons: per-member bookkeeping (step counter, monitor);
 // sync: batch_sync_words(nmembers) counters; err: the batch's error flag. Step s of the launch
 // reads buffer cur0 ^ (s & 1) of each member.
 size_t batch_sync_words(int nmembers);
-cudaError_t launch_batch_steps(int dtype, const void* members, const BatchMon* mons,
+cudaError_t launch_batch_steps(int dtype, int ty, const void* members, const BatchMon* mons,
                                const int2* items, int nitems, int nsteps, int grid, int packed,
                                unsigned* sync, int nmembers, unsigned* err, cudaStream_t st);
 

@@ -123,7 +123,7 @@ bool step2_box(int dtype, int d1, int ty, int* sw, int* ph, int* uh, int* hx, in
   return false;
 }
 
-int step2_occupancy(int, int) { return 1; }
+int step2_occupancy(int, int ty) { return ty == 16 ? 2 : 1; }
 
 template <int TY, bool PK, class TE> static cudaError_t prep2() {
   return cudaFuncSetAttribute(fslbm_step2_kernel<2, TY, PK, TE>,
@@ -173,7 +173,6 @@ cudaError_t launch_step2(const StepLaunch& a, const Step2Launch& b, cudaStream_t
   g.tiles = a.tiles; g.mask = a.mask; g.colcoef = a.colcoef; g.out = a.out;
   g.gauge = a.gauge; g.err = a.err;
   g.wb = a.wb; g.wgt = a.wgt;
-  g.wb = a.wb; g.wgt = a.wgt;
   g.step_counter = a.counters ? &a.counters->steps : nullptr;
   g.step_no = unsigned(a.step_no);
   StepConst<float> k;
@@ -214,21 +213,59 @@ __device__ void block_sum(double (&v)[NV], double* sh /* NV * 32 */) {
 // ------------------------------------------------------------------------------------------
 // The state is read through L2 (ld.global.cg): in a chained batched launch other CTAs of the
 // same grid wrote it, and this SM's L1 may hold lines of an earlier read of the same buffer.
-template <class TS>
+// The sums are formed in the order of a 512-thread block whatever the block size NT (512, or 256
+// in the batched kernel's 32 x 16 tile form, where each thread takes two of the 512 strands and
+// the warp partials of both), so every form books the same monitor record bit for bit.
+template <class TS, int NT = 512>
 __device__ void monitor_body(const MonitorLaunch& a, double* sh) {
   using TA = typename ArithOf<TS>::type;
+  static_assert(NT == 512 || NT == 256, "block of 256 or 512 threads");
   const TS* st = reinterpret_cast<const TS*>(a.state);
   const size_t FS = size_t(a.lxp) * a.ly * a.L;
   const TA pin = TA(a.pin);
   double v[3] = {0, 0, 0};   // sum w, sum p, sum (p - pin) over non-wall cells of plane z=0
-  for (int j = threadIdx.x; j < a.lxp * a.ly; j += blockDim.x) {
-    if (a.mask[j] != 0) continue;           // walls hold zero; periodic images are not counted
-    const TA p = TA(__ldcg(st + j));
-    v[0] += wval(__ldcg(st + 3 * FS + j), a.wb, size_t(j));
-    v[1] += double(p);
-    v[2] += double(TA(p - pin));            // the outlet buffer copy's p
+  auto strand = [&](int j0, double (&acc)[3]) {
+    for (int j = j0; j < a.lxp * a.ly; j += 512) {
+      if (a.mask[j] != 0) continue;         // walls hold zero; periodic images are not counted
+      const TA p = TA(__ldcg(st + j));
+      acc[0] += wval(__ldcg(st + 3 * FS + j), a.wb, size_t(j));
+      acc[1] += double(p);
+      acc[2] += double(TA(p - pin));        // the outlet buffer copy's p
+    }
+  };
+  if constexpr (NT == 512) {
+    for (int j = threadIdx.x; j < a.lxp * a.ly; j += blockDim.x) {
+      if (a.mask[j] != 0) continue;         // walls hold zero; periodic images are not counted
+      const TA p = TA(__ldcg(st + j));
+      v[0] += wval(__ldcg(st + 3 * FS + j), a.wb, size_t(j));
+      v[1] += double(p);
+      v[2] += double(TA(p - pin));          // the outlet buffer copy's p
+    }
+    block_sum<3>(v, sh);
+  } else {
+    // strands t and t + 256, each reduced over its warp as the 512-thread block's warps w and
+    // w + 8 reduce, then the 16 warp partials as block_sum's second stage adds them
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double u[3] = {0, 0, 0};
+    strand(threadIdx.x, v);
+    strand(threadIdx.x + 256, u);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      for (int o = 16; o > 0; o >>= 1) {
+        v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+        u[k] += __shfl_down_sync(0xffffffffu, u[k], o);
+      }
+      if (lane == 0) { sh[k * 32 + warp] = v[k]; sh[k * 32 + warp + 8] = u[k]; }
+    }
+    __syncthreads();
+    if (warp == 0)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        double s = lane < 16 ? sh[k * 32 + lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        v[k] = s;
+      }
   }
-  block_sum<3>(v, sh);
   if (threadIdx.x == 0) {
     const double q1 = v[0] / a.l1, p1 = v[1] / a.l1, p2 = v[2] / a.l1;
     fslbm_monitor r;
@@ -264,7 +301,7 @@ struct alignas(64) BatchMember {
   const double* gauge_slot;    // the member's monitor p2, applied on the step after a monitor
   const long long* steps;      // the member's device step counter
   long long stop_at;           // the member is not stepped once its counter reaches this
-  int w16x4;                   // warp shape of the member's items (16 x 4 instead of 32 x 2)
+  int shape;                   // warp shape of the member's items: 32 x 2, 16 x 4 or 8 x 8 (0, 1, 2)
   int monitor_every;
   int cur0;                    // input buffer at the launch's first step
 };
@@ -273,6 +310,7 @@ struct alignas(64) BatchMember {
 // the step's last item: the step counter advances (unless the member had reached its stop) and,
 // when due, the monitor record and the gauge of the member's next step are written. Inlined: any
 // call in the batched kernel makes its march spill registers (the call ABI).
+template <int NT>
 __device__ __forceinline__ void batch_book(const BatchMon& b, int parity_after, double* sh, int* due) {
   if (threadIdx.x == 0) {
     const long long s0 = __ldcg(&b.mon.counters->steps);
@@ -287,8 +325,8 @@ __device__ __forceinline__ void batch_book(const BatchMon& b, int parity_after, 
   if (*due) {
     MonitorLaunch a = b.mon;
     a.state = b.state[b.cur0 ^ parity_after];
-    if (a.dtype == FSLBM_F16) monitor_body<__half>(a, sh);
-    else monitor_body<float>(a, sh);
+    if (a.dtype == FSLBM_F16) monitor_body<__half, NT>(a, sh);
+    else monitor_body<float, NT>(a, sh);
   }
 }
 
@@ -334,7 +372,7 @@ __device__ __forceinline__ bool batch_item_begin(const BatchMember& mb, int memb
 // and releases it before marching on. Counting there rather than right after the march keeps
 // the march free of register spills.
 template <int D1, int TY, bool PK, class TE>
-__global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
+__global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, TY == 16 ? 2 : 1)
     fslbm_step2_batch_kernel(const BatchMember* __restrict__ members,
                              const BatchMon* __restrict__ mons, const int2* __restrict__ items,
                              int nitems, int nsteps, unsigned* sync, unsigned* err) {
@@ -370,7 +408,7 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
       const unsigned pt = unsigned(s_book);
       const int pm = items[pt % unsigned(nitems)].x;
       const int ps = int(pt / unsigned(nitems));
-      batch_book(mons[pm], (ps & 1) ^ 1, s_sh, &s_due);
+      batch_book<Step2Tile<D1, TY, TE>::THREADS>(mons[pm], (ps & 1) ^ 1, s_sh, &s_due);
       __threadfence();
       __syncthreads();
       if (threadIdx.x == 0) st_release_gpu(sync + 5 + 2 * pm, unsigned(ps + 1));
@@ -389,29 +427,29 @@ __global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
       const int ntiles = mb.g.ntiles;
       const bool ok = step2_march<D1, TY, PK, TE>(&mb.map_p[cur], &mb.map_u[cur], s_g, s_k,
                                                   it.y % ntiles, it.y / ntiles, smem, !first,
-                                                  mb.w16x4 != 0);
+                                                  mb.shape);
       if (!ok) return;
       first = false;
     }
   }
 }
 
-template <bool PK, class TE> static cudaError_t batch_prep() {
-  return cudaFuncSetAttribute(fslbm_step2_batch_kernel<2, 32, PK, TE>,
+template <int TY, bool PK, class TE> static cudaError_t batch_prep() {
+  return cudaFuncSetAttribute(fslbm_step2_batch_kernel<2, TY, PK, TE>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(Step2Tile<2, 32, TE>::SMEM_BYTES));
+                              int(Step2Tile<2, TY, TE>::SMEM_BYTES));
 }
 
-cudaError_t batch_prepare(int dtype) {
+template <int TY, class TE> static cudaError_t batch_prep_all() {
   cudaError_t e;
-  if (dtype == FSLBM_F32) {
-    if ((e = batch_prep<true, float>())) return e;
-    return batch_prep<false, float>();
-  }
-  if (dtype == FSLBM_F16) {
-    if ((e = batch_prep<true, __half>())) return e;
-    return batch_prep<false, __half>();
-  }
+  if ((e = batch_prep<TY, true, TE>())) return e;
+  return batch_prep<TY, false, TE>();
+}
+
+cudaError_t batch_prepare(int dtype, int ty) {
+  if (ty != 16 && ty != 32) return cudaErrorInvalidValue;
+  if (dtype == FSLBM_F32) return ty == 16 ? batch_prep_all<16, float>() : batch_prep_all<32, float>();
+  if (dtype == FSLBM_F16) return ty == 16 ? batch_prep_all<16, __half>() : batch_prep_all<32, __half>();
   return cudaErrorInvalidValue;
 }
 
@@ -420,7 +458,7 @@ size_t batch_member_bytes() { return sizeof(BatchMember); }
 cudaError_t fill_batch_member(void* dst, const CUtensorMap* mp, const CUtensorMap* mu,
                               const StepLaunch& a, void* state0, void* state1,
                               const double* gauge_slot, const long long* steps, long long stop_at,
-                              int monitor_every, int cur0, int nchunks, int w16x4) {
+                              int monitor_every, int cur0, int nchunks, int shape) {
   BatchMember m;
   std::memset(&m, 0, sizeof m);
   m.map_p[0] = mp[0]; m.map_p[1] = mp[1];
@@ -433,36 +471,38 @@ cudaError_t fill_batch_member(void* dst, const CUtensorMap* mp, const CUtensorMa
   m.k.m = float(a.m); m.k.c0 = float(a.c0); m.k.c1 = float(a.c1); m.k.c2 = float(a.c2);
   m.k.fx = float(a.fx); m.k.fy = float(a.fy); m.k.fz = float(a.fz);
   m.state[0] = state0; m.state[1] = state1;
-  m.gauge_slot = gauge_slot; m.steps = steps; m.stop_at = stop_at; m.w16x4 = w16x4;
+  m.gauge_slot = gauge_slot; m.steps = steps; m.stop_at = stop_at; m.shape = shape;
   m.monitor_every = monitor_every; m.cur0 = cur0;
   std::memcpy(dst, &m, sizeof m);
   return cudaSuccess;
 }
 
-template <class TE>
+template <int TY, class TE>
 static void launch_batch_t(const BatchMember* mb, const BatchMon* mons, const int2* items,
                            int nitems, int nsteps, int grid, int packed, unsigned* sync,
                            unsigned* err, cudaStream_t st) {
-  using Tl = Step2Tile<2, 32, TE>;
+  using Tl = Step2Tile<2, TY, TE>;
   if (packed)
-    fslbm_step2_batch_kernel<2, 32, true, TE><<<grid, Tl::THREADS, Tl::SMEM_BYTES, st>>>(
+    fslbm_step2_batch_kernel<2, TY, true, TE><<<grid, Tl::THREADS, Tl::SMEM_BYTES, st>>>(
         mb, mons, items, nitems, nsteps, sync, err);
   else
-    fslbm_step2_batch_kernel<2, 32, false, TE><<<grid, Tl::THREADS, Tl::SMEM_BYTES, st>>>(
+    fslbm_step2_batch_kernel<2, TY, false, TE><<<grid, Tl::THREADS, Tl::SMEM_BYTES, st>>>(
         mb, mons, items, nitems, nsteps, sync, err);
 }
 
 size_t batch_sync_words(int nmembers) { return 4 + 2 * size_t(nmembers); }
 
-cudaError_t launch_batch_steps(int dtype, const void* members, const BatchMon* mons,
+cudaError_t launch_batch_steps(int dtype, int ty, const void* members, const BatchMon* mons,
                                const int2* items, int nitems, int nsteps, int grid, int packed,
                                unsigned* sync, int nmembers, unsigned* err, cudaStream_t st) {
   if (nsteps < 1) return cudaSuccess;
   cudaError_t e = cudaMemsetAsync(sync, 0, batch_sync_words(nmembers) * sizeof(unsigned), st);
   if (e) return e;
   const BatchMember* mb = reinterpret_cast<const BatchMember*>(members);
-  if (dtype == FSLBM_F32) launch_batch_t<float>(mb, mons, items, nitems, nsteps, grid, packed, sync, err, st);
-  else if (dtype == FSLBM_F16) launch_batch_t<__half>(mb, mons, items, nitems, nsteps, grid, packed, sync, err, st);
+  if (ty == 32 && dtype == FSLBM_F32) launch_batch_t<32, float>(mb, mons, items, nitems, nsteps, grid, packed, sync, err, st);
+  else if (ty == 32 && dtype == FSLBM_F16) launch_batch_t<32, __half>(mb, mons, items, nitems, nsteps, grid, packed, sync, err, st);
+  else if (ty == 16 && dtype == FSLBM_F32) launch_batch_t<16, float>(mb, mons, items, nitems, nsteps, grid, packed, sync, err, st);
+  else if (ty == 16 && dtype == FSLBM_F16) launch_batch_t<16, __half>(mb, mons, items, nitems, nsteps, grid, packed, sync, err, st);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }

@@ -5,9 +5,10 @@
 //  - every thread owns two adjacent columns (x, x+1) and computes both with packed FP32x2
 //    arithmetic (__ffma2_rn / __fadd2_rn / __fmul2_rn); neighbour pairs come from 64-bit
 //    shared-memory loads;
-//  - a 32 x TY tile per CTA (512 threads for TY = 32, 16 warps per SM); p is staged with a
-//    one-cell halo, u,v,w with the corrector's 2*d1 halo, as two TMA boxes per plane into a
-//    window of 8 planes (output plane .. 3 planes ahead for d1 = 2);
+//  - a 32 x TY tile per CTA, 16 warps per SM either way (TY = 32: one 512-thread CTA per SM;
+//    TY = 16: two 256-thread CTAs, which suit small cross-sections); p is staged with a one-cell
+//    halo, u,v,w with the corrector's 2*d1 halo, as two TMA boxes per plane into a window of 8
+//    planes for TY = 32 (output plane .. 3 planes ahead for d1 = 2), 7 for TY = 16;
 //  - no block-wide barrier in the march and no producer thread: per-slot "full" mbarriers count
 //    TMA completion, each warp releases a slot after its last read of the plane in it, and the
 //    last warp to release a slot refills it, so warps drift within the window and none waits
@@ -48,7 +49,9 @@ template <int D1, int TY, class TE = float> struct Step2Tile {
   static constexpr int PPLANE = (SW * PH * ES + 127) / 128 * 128 / ES;   // 128-byte aligned
   static constexpr int UPLANE = SW * UH;
   static constexpr int SLOT = PPLANE + 3 * UPLANE;
-  static constexpr int S = 8;                           // window slots (power of two)
+  // window slots: 8 for 32 x 32 tiles (one 512-thread CTA per SM), 7 for 32 x 16 tiles, so that
+  // two 256-thread CTAs fit an SM's shared memory
+  static constexpr int S = TY == 16 ? 7 : 8;
   static constexpr int AHEAD = S - R - 1;               // planes loaded beyond the current one
   static_assert(AHEAD >= 1, "window too small for the corrector reach");
   static constexpr uint32_t TX_BYTES = uint32_t((SW * PH + 3 * UPLANE) * ES);
@@ -187,35 +190,46 @@ __device__ __forceinline__ float2 qof(float2 P, float2 U, float2 V, float2 W) {
 // Freed window slots are refilled by the last warp to release them (no warp waits for a free
 // slot); measured +2 % on the single pipe and +1.7 % on the batched ensemble against thread 0
 // waiting on per-slot "empty" mbarriers and refilling.
-// The warp shape (w16x4, below) is a runtime argument: it only places each thread in the tile, and
-// a kernel that inlines one march for both shapes (the batched kernel, whose members choose
-// their shape) keeps one copy of the march instead of two, which ended its register spills.
+// The warp shape (below) is a runtime argument: it only places each thread in the tile, and a
+// kernel that inlines one march for every shape (the batched kernel, whose members choose their
+// shape) keeps one copy of the march instead of one per shape, which ended its register spills.
 template <int D1, int TY, bool PK, class TE>
 __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUtensorMap* tmap_uvw,
                                             const Step2Geom& g, const StepConst<float>& k,
                                             int tile, int chunk, unsigned char* smem, bool reinit,
-                                            bool w16x4 = false) {
+                                            int shape = 0) {
   using Tl = Step2Tile<D1, TY, TE>;
   using F = Pair<PK>;
   static_assert(D1 == 2, "the march prologue below is written for d1 = 2 (R = 4)");
   constexpr int R = Tl::R, HX = Tl::HX, HY = Tl::HY, SW = Tl::SW, S = Tl::S;
   constexpr int PPL = Tl::PPLANE, UPL = Tl::UPLANE, SLOT = Tl::SLOT;
 
+  // window slot of march plane m and the parity of its fill (m >= 0)
+  auto slot_of = [](int m) { return int(unsigned(m) % unsigned(S)); };
+  auto phase_of = [](int m) { return uint32_t((unsigned(m) / unsigned(S)) & 1u); };
   TE* ring = reinterpret_cast<TE*>(smem);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + Tl::BAR_OFFSET);
   // per slot: warp releases, counted to elect the refilling warp
   unsigned* released = reinterpret_cast<unsigned*>(full + S);
 
-  // Warp shape. Default: 32 columns x 2 rows (each half-warp reads one contiguous row).
-  // w16x4: 16 columns (8 pairs) x 4 rows, so warps over wall skip at a finer grain, which pays
-  // for small cross-sections (measured +6 % on the mixed-size ensemble, -2 % on the 128 x 128
-  // pipe). There lanes 0-15 take rows 0 and 2 of the warp and lanes 16-31 rows 1 and 3: with the
-  // 160-byte FP32 row stride each half-warp's 64-bit shared loads fall on distinct banks (FP16
-  // rows of 96 bytes are conflict-free in any order). The map changes no thread's arithmetic.
-  static_assert(Tl::TX == 32 && TY % 4 == 0, "warp shapes within a 32-wide tile");
+  // Warp shape. 0: 32 columns x 2 rows (each half-warp reads one contiguous row); 1: 16 columns
+  // (8 pairs) x 4 rows; 2: 8 columns (4 pairs) x 8 rows. The smaller shapes let warps over wall
+  // skip at a finer grain, which pays for small cross-sections (16 x 4: measured +6 % on the
+  // mixed-size ensemble, -2 % on the 128 x 128 pipe). 16 x 4: lanes 0-15 take rows 0 and 2 of
+  // the warp, lanes 16-31 rows 1 and 3; 8 x 8: lanes 4r .. 4r+3 take row r. With the 160-byte
+  // FP32 row stride each half-warp's 64-bit shared loads fall on distinct banks in every shape
+  // (FP16 rows of 96 bytes: conflict-free for 32 x 2 and 16 x 4, two-way for 8 x 8). The map
+  // changes no thread's arithmetic.
+  static_assert(Tl::TX == 32 && TY % 8 == 0, "warp shapes within a 32-wide tile");
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int tp = w16x4 ? (warp & 1) * 8 + (lane & 7) : tid % (Tl::TX / 2);
-  const int ty = w16x4 ? (warp >> 1) * 4 + ((lane >> 3) & 1) * 2 + (lane >> 4) : tid / (Tl::TX / 2);
+  int tp = tid % (Tl::TX / 2), ty = tid / (Tl::TX / 2);
+  if (shape == 1) {
+    tp = (warp & 1) * 8 + (lane & 7);
+    ty = (warp >> 1) * 4 + ((lane >> 3) & 1) * 2 + (lane >> 4);
+  } else if (shape == 2) {
+    tp = (warp & 3) * 4 + (lane & 3);
+    ty = (warp >> 2) * 8 + (lane >> 2);
+  }
 
   // ---- work: one (tile, chunk); odd chunks march towards -z
   const int zb = int((long long)g.L * chunk / g.nchunks);
@@ -256,7 +270,7 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
   __syncthreads();
 
   auto issue = [&](int m) {            // load march plane m into slot m % S
-    const int slot = m & (S - 1);
+    const int slot = slot_of(m);
     int zz = (start + dir * m) % g.L;
     if (zz < 0) zz += g.L;
     TE* dst = ring + slot * SLOT;
@@ -273,11 +287,11 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
   auto drain = [&](int from) {
     if (lane == 0)
       for (int q = from; q < niter && q < from + S; ++q)
-        mbar_wait_bounded(&full[q & (S - 1)], uint32_t((q / S) & 1), kWaitLimitNs / 8);
+        mbar_wait_bounded(&full[slot_of(q)], phase_of(q), kWaitLimitNs / 8);
   };
   // wait for march plane m; false after flagging a failure (the caller returns)
   auto arrive_wait = [&](int m) -> bool {
-    if (mbar_wait_bounded(&full[m & (S - 1)], uint32_t((m / S) & 1), kWaitLimitNs)) return true;
+    if (mbar_wait_bounded(&full[slot_of(m)], phase_of(m), kWaitLimitNs)) return true;
     if (lane == 0) atomicOr(g.err, 1u);
     drain(m + 1);
     return false;
@@ -291,7 +305,7 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
   auto release_produce = [&](int m) -> bool {
     __syncwarp();
     if (m >= R && lane == 0) {
-      const int slot = (m - R) & (S - 1);
+      const int slot = slot_of(m - R);
       const unsigned seen = atom_add_acq_rel_cta(&released[slot], 1u) + 1u;
       const int mn = m - R + S;
       if (seen % unsigned(Tl::WARPS) == 0u && mn < niter) {
@@ -349,7 +363,7 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
 
   // predictor contribution of march plane ma (see step_kernel.cuh for the factorisation)
   auto predictor = [&](int ma) {
-    const TE* ss = ring + (ma & (S - 1)) * SLOT;
+    const TE* ss = ring + slot_of(ma) * SLOT;
     const int sp = start + dir * ma;                          // real plane
     const float off = sp < 0 ? k.pin : (sp >= g.L ? -k.pin : 0.0f);
     // Row-factored weights w(cx)w(cy) = {4,1,1}x{4,1,1}/36, per column of the pair: per row
@@ -462,7 +476,7 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
 
   // own columns of march plane jo (for the history)
   auto own = [&](int jo, float2& uc, float2& vc, float2& wc) {
-    const TE* so = ring + (jo & (S - 1)) * SLOT;
+    const TE* so = ring + slot_of(jo) * SLOT;
     uc = lds2(so + uo); vc = lds2(so + uo + UPL); wc = lds2(so + uo + 2 * UPL);
   };
 
@@ -470,9 +484,9 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
   // overwritten with plane jo
   auto output = [&](int jo, auto rot_c) {
     constexpr int ROT = decltype(rot_c)::value;
-    const TE* so = ring + (jo & (S - 1)) * SLOT;
-    const TE* sa1 = ring + ((jo + D1) & (S - 1)) * SLOT;   // march planes ahead
-    const TE* sa2 = ring + ((jo + 2 * D1) & (S - 1)) * SLOT;
+    const TE* so = ring + slot_of(jo) * SLOT;
+    const TE* sa1 = ring + slot_of(jo + D1) * SLOT;   // march planes ahead
+    const TE* sa2 = ring + slot_of(jo + 2 * D1) * SLOT;
     const float2 pc = lds2(so + po);
     const float2 uc = lds2(so + uo), vc = lds2(so + uo + UPL), wc = lds2(so + uo + 2 * UPL);
     // u_new = K1 t1 + K2 t2 + K0 u + tb m* + tb F
@@ -555,14 +569,14 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
 
 // One pipe, one step: CTA b marches (tile b % ntiles, chunk b / ntiles).
 template <int D1, int TY, bool PK, class TE>
-__global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, 1)
+__global__ void __launch_bounds__(Step2Tile<D1, TY, TE>::THREADS, TY == 16 ? 2 : 1)
     fslbm_step2_kernel(const __grid_constant__ CUtensorMap tmap_p,
                        const __grid_constant__ CUtensorMap tmap_uvw, const Step2Geom g,
                        const StepConst<float> k) {
   extern __shared__ __align__(128) unsigned char smem[];
   if (threadIdx.x == 0 && blockIdx.x == 0 && g.step_counter) *g.step_counter += 1;
   step2_march<D1, TY, PK, TE>(&tmap_p, &tmap_uvw, g, k, blockIdx.x % g.ntiles,
-                          blockIdx.x / g.ntiles, smem, false);
+                              blockIdx.x / g.ntiles, smem, false);
 }
 
 }  // namespace fslbm

@@ -224,14 +224,17 @@ int fslbm_batch_elapsed(fslbm_batch* b, double* ms);
  * the others keep stepping. */
 int fslbm_batch_set_stop(fslbm_batch* b, int member, int64_t stop_step);
 /* Batch tiling (no reference counterpart). A member's work items span `chunk` streamwise planes
- * (each chunk re-reads 2*2*d1 halo planes) and use warps of 16 x 4 cells (warp16x4 = 1) or
- * 32 x 2 cells (0). Members fall in size classes (32-wide tiles across x and y, length rounded
- * up to a power of two); a batch takes its classes' tiling from the table named by the
- * FSLBM_BATCH_TUNING environment variable, else from batch_tiling.json next to the library,
- * else 64 planes and 16 x 4 warps. */
-int fslbm_batch_set_tiling(fslbm_batch* b, int member, int chunk, int warp16x4);
+ * (each chunk re-reads 2*2*d1 halo planes) and use warps of 32 x 2 cells (warp_shape = 0),
+ * 16 x 4 cells (1) or 8 x 8 cells (2); warps whose cells are all wall skip the arithmetic, so
+ * the smaller shapes suit small cross-sections. Members fall in size classes (32-wide tiles
+ * across x and y, length rounded up to a power of two); a batch takes its classes' tiling from
+ * the table named by the FSLBM_BATCH_TUNING environment variable, else from batch_tiling.json
+ * next to the library, else 128 planes and 16 x 4 warps. The batch marches its own 32 x 16
+ * column tiles (two CTAs per SM; FSLBM_BATCH_TILE_Y=32 selects 32 x 32 tiles), independent of
+ * the tiling each member uses when stepped alone. */
+int fslbm_batch_set_tiling(fslbm_batch* b, int member, int chunk, int warp_shape);
 int fslbm_batch_load_tiling(fslbm_batch* b, const char* path);
-/* Autotuner: times each size class's candidate tilings (chunks 16..256, both warp shapes) on the
+/* Autotuner: times each size class's candidate tilings (chunks 16..256, the three warp shapes) on the
  * batch itself, trial_steps steps per candidate, keeps the fastest per class, restores every
  * member's fields, step count, monitor log and gauge, and writes the table to `path` (JSON) if
  * not NULL. Needs members on the batched kernel (FP32 or FP16 storage, d1 = 2). If a member's

@@ -75,6 +75,40 @@ def test_batch_matches_members_alone(built, ctx, use_graph, dtype):
         s.close()
 
 
+@pytest.mark.parametrize("tile_y,shape", [(16, 0), (16, 2), (32, 1), (32, 2)])
+def test_batch_tile_heights_and_warp_shapes(built, ctx, monkeypatch, tile_y, shape):
+    """The batch's own tile height (32 x 16 tiles, two CTAs per SM, or 32 x 32) and warp shape
+    (32 x 2, 16 x 4 or 8 x 8 cells) place the threads differently but change no cell's
+    arithmetic, and the batched monitor sums in the same order at either block size: fields and
+    monitor records equal the members stepped alone, bit for bit."""
+    monkeypatch.setenv("FSLBM_BATCH_TILE_Y", str(tile_y))
+    fb = built
+    specs = member_specs(n=4, seed=7)
+    steps = 30
+    alone = []
+    for sp in specs:
+        s = make_member(fb, ctx, sp)
+        s.step(steps)
+        s.sync()
+        alone.append((s.get_fields(np.float32), s.monitor_log()))
+        s.close()
+    members = [make_member(fb, ctx, sp) for sp in specs]
+    b = fb.Batch(ctx, members)
+    for i in range(len(members)):
+        b.set_tiling(i, 48, shape)
+    b.step(steps)
+    b.sync()
+    for s, (want, wlog) in zip(members, alone):
+        assert np.array_equal(s.get_fields(np.float32), want)
+        glog = s.monitor_log()
+        assert len(glog) == len(wlog) == 1
+        for key in ("q1", "p1", "p2", "sample"):
+            assert glog[0][key] == wlog[0][key], key
+    b.close()
+    for s in members:
+        s.close()
+
+
 def test_batch_member_stops(built, ctx):
     """Members with different step budgets share launches; each stops at its own budget and
     equals the member stepped alone for that many steps."""
@@ -122,7 +156,8 @@ def test_autotune_restores_state_and_keeps_results(built, ctx, tmp_path):
     b = fb.Batch(ctx, members)
     path = str(tmp_path / "tiling.json")
     table = b.autotune(trial_steps=4, path=path)
-    assert table and all(set(v) >= {"chunk", "warp16x4"} for v in table.values())
+    assert table and all(set(v) >= {"chunk", "warp_shape"} for v in table.values())
+    assert all(v["warp_shape"] in (0, 1, 2) for v in table.values())
     assert json.load(open(path))["format"] == "fslbm batch tiling 1"
     for s in members:
         assert s.info()["steps"] == 0 and s.monitor_log() == []
