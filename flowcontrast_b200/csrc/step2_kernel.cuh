@@ -296,21 +296,27 @@ __device__ __forceinline__ bool step2_march(const CUtensorMap* tmap_p, const CUt
     drain(m + 1);
     return false;
   };
-  // Plane m - R leaves the window and its slot takes plane m - R + S (= m + AHEAD + 1).
-  // __syncwarp orders the warp's shared loads before lane 0's acq_rel add to the slot's counter;
-  // the warp whose add completes the count has acquired every warp's loads and orders them
-  // before its TMA write with a proxy fence. A slot's next cycle starts only after its refill
-  // lands, which needs all WARPS releases of this cycle, so the count is a multiple of WARPS
-  // exactly when a cycle is complete.
+  // Plane m - R leaves the window at iteration m (its last reader is output(m - R)). Planes leave
+  // in pairs: at odd p = m - R, planes p - 1 and p, whose slots take planes p - 1 + S and p + S.
+  // __syncwarp orders the warp's shared loads before lane 0's acq_rel add to the pair's counter
+  // (the slot of plane p); the warp whose add completes the count has acquired every warp's loads
+  // and orders them before its TMA writes with a proxy fence. One add per two planes halves the
+  // release cost, which is a fence-like wait (measured: plain step +1.5 %, batched ensemble +9 %).
+  // Plane m fills the slot of plane m - S, so a warp waiting for plane m needs every warp to have
+  // released at iteration m - AHEAD at the latest (instead of m - AHEAD - 1): an earlier
+  // iteration, as AHEAD >= 1, so no wait depends on itself. A counter's next use (2S planes later
+  // for odd S, S for S = 8) comes only after every warp has passed its previous use, so the count
+  // is a multiple of WARPS exactly when a pair is complete.
   auto release_produce = [&](int m) -> bool {
     __syncwarp();
-    if (m >= R && lane == 0) {
+    if (m >= R && ((m - R) & 1) && lane == 0) {
       const int slot = slot_of(m - R);
       const unsigned seen = atom_add_acq_rel_cta(&released[slot], 1u) + 1u;
-      const int mn = m - R + S;
+      const int mn = m - R + S - 1;
       if (seen % unsigned(Tl::WARPS) == 0u && mn < niter) {
         fence_proxy_async_smem();
         issue(mn);
+        if (mn + 1 < niter) issue(mn + 1);
       }
     }
     return true;
