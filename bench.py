@@ -394,6 +394,15 @@ def _member_start(fb, s, sp):
     s.init_poiseuille(2 * wl.U_BULK, noise=1e-3, modes=4, mode_amp=0.05, seed=sp.seed)
 
 
+def batch_kernel_name(storage):
+    """The batched kernel the library launches: 32 x 16 tiles unless FSLBM_BATCH_TILE_Y=32,
+    packed pair arithmetic unless FSLBM_BATCH_PACKED=0."""
+    ty = 32 if os.environ.get("FSLBM_BATCH_TILE_Y") == "32" else 16
+    form = "scalar" if os.environ.get("FSLBM_BATCH_PACKED") == "0" else "packed"
+    te = "__half" if storage == "f16" else "float"
+    return f"fslbm_step2_batch_kernel<2,{ty},{form},{te}> (chained steps)"
+
+
 def run_ensemble(args):
     """Mixed-size ensemble (64 seeded pipes, L in [32,256], n in [24,96], Re in [50,3000]):
     the batched persistent launch (FP32 storage, or FP16 storage with --ensemble-dtype f16)
@@ -514,7 +523,7 @@ def run_ensemble(args):
                          "frac": achieved / peak,
                          "traffic": None,
                          "peak_source": f"{peak_kind} hbm_gbs",
-                         "kernel": "fslbm_step2_batch_kernel<2,32,packed,float> (chained steps)"},
+                         "kernel": batch_kernel_name(args.ensemble_dtype)},
             "e2e": {"value": cells * args.steps / e2e_s / 1e6, "unit": "MLUPS",
                     "h2d_bytes_per_step": 16.0 * cells / args.steps,
                     "d2h_bytes_per_step": 16.0 * cells / args.steps},
