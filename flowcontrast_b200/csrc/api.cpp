@@ -273,8 +273,9 @@ static int validate_params(const fslbm_params* p, int dtype) {
 static int encode_pair_maps(const fslbm_solve* s, int ty, CUtensorMap mp[2], CUtensorMap mu[2]) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return fslbm_set_error(FSLBM_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
-  const CUtensorMapDataType dt = s->dtype == FSLBM_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
-                                                       : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const CUtensorMapDataType dt = s->dtype == FSLBM_F64   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                 : s->dtype == FSLBM_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   int sw2, ph, uh, hx2, hy2;
   if (!step2_box(s->dtype, s->prm.d1, ty, &sw2, &ph, &uh, &hx2, &hy2))
     return fslbm_set_error(FSLBM_ERR_ARG, "no column-pair kernel for d1 %d, tile height %d", s->prm.d1, ty);
@@ -372,7 +373,8 @@ static int configure_kernel(fslbm_solve* s) {
   // FP16 storage exists only in the column-pair kernel, which has the 2-tap corrector
   s->use2 = step2_supported(s->dtype, s->prm.d1) && s->K == 2 && s->planes == 1 &&
             (s->dtype == FSLBM_F16 || !(ek && std::atoi(ek) == 1));
-  s->ty2 = (et && std::atoi(et) == 16) ? 16 : 32;
+  // FP64 runs the column kernel on 32 x 16 tiles
+  s->ty2 = (s->dtype == FSLBM_F64 || (et && std::atoi(et) == 16)) ? 16 : 32;
   const char* ep = std::getenv("FSLBM_PACKED");
   s->packed2 = (ep && std::atoi(ep) == 0) ? 0 : 1;
   const std::vector<int2> tiles = fluid_tiles(s, s->use2 ? s->ty2 : kTY);
@@ -393,7 +395,7 @@ static int configure_kernel(fslbm_solve* s) {
     // tiles x streamwise chunks, at most one CTA per SM slot and chunks of at least 2R planes
     // (chunk counts weighted by each tile's fluid warps measured no faster: a tile with wall in
     // it is not proportionally faster per plane)
-    const int slots = s->ctx->sm_count * step2_occupancy(s->prm.d1, s->ty2);
+    const int slots = s->ctx->sm_count * step2_occupancy(s->dtype, s->prm.d1, s->ty2);
     int nch = std::max(1, slots / s->ntiles);
     nch = std::min(nch, std::max(1, s->L / (4 * s->prm.d1)));
     s->grid2 = s->ntiles * nch;
@@ -1346,7 +1348,7 @@ static int64_t item_cost(const fslbm_solve* s, const std::vector<int> (&warps)[3
 
 // Resident CTAs of the batched kernel: one per SM for 32 x 32 tiles, two for 32 x 16 tiles.
 static int batch_slots(const fslbm_batch* b) {
-  return b->ctx->sm_count * step2_occupancy(2, b->ty);
+  return b->ctx->sm_count * step2_occupancy(b->members[0]->dtype, 2, b->ty);
 }
 
 // Streamwise chunks of a member: about `chunk` planes each, at least 4*d1 planes.
@@ -1369,7 +1371,8 @@ static int batch_upload(fslbm_batch* b) {
   // (stride, corrector order or storage type changed) is refused
   for (int i = 0; i < n; ++i) {
     const fslbm_solve* s = b->members[i];
-    if (!(s->use2 && s->prm.d1 == 2 && s->dtype == b->members[0]->dtype && s->nghost == 0))
+    if (!(s->use2 && s->prm.d1 == 2 && s->dtype == b->members[0]->dtype && s->dtype != FSLBM_F64 &&
+          s->nghost == 0))
       return fslbm_set_error(FSLBM_ERR_STATE, "batch_step: member %d was reconfigured and no longer "
                              "fits the batched kernel; create a new batch", i);
   }
@@ -1566,7 +1569,7 @@ extern "C" int fslbm_batch_create(fslbm_ctx* ctx, fslbm_solve* const* solves, in
     b->stop.push_back(-1);
     b->m_chunk.push_back(128);
     b->m_shape.push_back(1);
-    fast = fast && solves[i]->use2 && solves[i]->prm.d1 == 2 &&
+    fast = fast && solves[i]->use2 && solves[i]->prm.d1 == 2 && solves[i]->dtype != FSLBM_F64 &&
            solves[i]->dtype == solves[0]->dtype && solves[i]->nghost == 0;
   }
   b->fast = fast;

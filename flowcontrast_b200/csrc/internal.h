@@ -59,8 +59,9 @@ bool step_supported(int dtype, int d1, int K);
 cudaError_t step_prepare(int dtype, int d1, int K);   // sets the dynamic shared memory attribute
 cudaError_t launch_step(const StepLaunch& a, cudaStream_t st);
 
-// FP32 column-pair kernel (even d1): two tensor maps per input state (p box with a one-cell
-// halo, u,v,w box with the corrector halo) and a persistent grid.
+// Column-pair kernel (FP32 / FP16 storage, d1 = 2) and FP64 column kernel (d1 = 2, 32 x 16
+// tiles): two tensor maps per input state (p box with a one-cell halo, u,v,w box with the
+// corrector halo).
 struct Step2Launch {
   int d1, ty;                // corrective stride, tile height (16 or 32)
   int packed;                // FP32x2 packed arithmetic (1) or scalar pairs (0)
@@ -70,7 +71,7 @@ struct Step2Launch {
 };
 bool step2_supported(int dtype, int d1);
 bool step2_box(int dtype, int d1, int ty, int* sw, int* ph, int* uh, int* hx, int* hy);
-int step2_occupancy(int d1, int ty);   // CTAs per SM the kernel is built for
+int step2_occupancy(int dtype, int d1, int ty);   // CTAs per SM the kernel is built for
 cudaError_t step2_prepare(int dtype, int d1, int ty);
 cudaError_t launch_step2(const StepLaunch& a, const Step2Launch& b, cudaStream_t st);
 

@@ -6,6 +6,7 @@
 #include "internal.h"
 #include "step_kernel.cuh"
 #include "step2_kernel.cuh"
+#include "stepcol_kernel.cuh"
 
 namespace fslbm {
 
@@ -97,10 +98,10 @@ cudaError_t launch_step(const StepLaunch& a, cudaStream_t st) {
 }
 
 // ------------------------------------------------------------------------------------------
-// FP32 column-pair kernel dispatch
+// column-pair kernel (FP32 / FP16 storage) and FP64 column kernel dispatch
 // ------------------------------------------------------------------------------------------
 bool step2_supported(int dtype, int d1) {
-  return (dtype == FSLBM_F32 || dtype == FSLBM_F16) && d1 == 2;
+  return (dtype == FSLBM_F32 || dtype == FSLBM_F16 || dtype == FSLBM_F64) && d1 == 2;
 }
 
 template <int TY, class TE> static void box2(int* sw, int* ph, int* uh, int* hx, int* hy) {
@@ -110,6 +111,12 @@ template <int TY, class TE> static void box2(int* sw, int* ph, int* uh, int* hx,
 
 bool step2_box(int dtype, int d1, int ty, int* sw, int* ph, int* uh, int* hx, int* hy) {
   if (d1 != 2 || (ty != 32 && ty != 16)) return false;
+  if (dtype == FSLBM_F64) {          // the FP64 column kernel: 32 x 16 tiles only
+    using Tl = ColTile<2, 16>;
+    if (ty != 16) return false;
+    *sw = Tl::SW; *ph = Tl::PH; *uh = Tl::UH; *hx = Tl::HX; *hy = Tl::HY;
+    return true;
+  }
   if (dtype == FSLBM_F32) {
     if (ty == 32) box2<32, float>(sw, ph, uh, hx, hy);
     else box2<16, float>(sw, ph, uh, hx, hy);
@@ -123,7 +130,7 @@ bool step2_box(int dtype, int d1, int ty, int* sw, int* ph, int* uh, int* hx, in
   return false;
 }
 
-int step2_occupancy(int, int ty) { return ty == 16 ? 2 : 1; }
+int step2_occupancy(int dtype, int, int ty) { return dtype != FSLBM_F64 && ty == 16 ? 2 : 1; }
 
 template <int TY, bool PK, class TE> static cudaError_t prep2() {
   return cudaFuncSetAttribute(fslbm_step2_kernel<2, TY, PK, TE>,
@@ -146,6 +153,10 @@ template <class TE> static cudaError_t prep2_all(int ty) {
 
 cudaError_t step2_prepare(int dtype, int d1, int ty) {
   if (d1 != 2) return cudaErrorInvalidValue;
+  if (dtype == FSLBM_F64)
+    return ty != 16 ? cudaErrorInvalidValue
+                    : cudaFuncSetAttribute(fslbm_col_kernel<2, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           int(ColTile<2, 16>::SMEM_BYTES));
   if (dtype == FSLBM_F32) return prep2_all<float>(ty);
   if (dtype == FSLBM_F16) return prep2_all<__half>(ty);
   return cudaErrorInvalidValue;
@@ -180,6 +191,16 @@ cudaError_t launch_step2(const StepLaunch& a, const Step2Launch& b, cudaStream_t
   k.m = float(a.m); k.c0 = float(a.c0); k.c1 = float(a.c1); k.c2 = float(a.c2);
   k.fx = float(a.fx); k.fy = float(a.fy); k.fz = float(a.fz);
   if (b.d1 != 2) return cudaErrorInvalidValue;
+  if (a.dtype == FSLBM_F64) {
+    if (b.ty != 16) return cudaErrorInvalidValue;
+    StepConst<double> kd;
+    kd.tb = a.tb; kd.cc = a.cc; kd.pin = a.pin; kd.dtddy = a.dtddy; kd.m = a.m;
+    kd.c0 = a.c0; kd.c1 = a.c1; kd.c2 = a.c2; kd.fx = a.fx; kd.fy = a.fy; kd.fz = a.fz;
+    for (int j = 0; j < 6; ++j) kd.ch[j] = a.ch[j];
+    fslbm_col_kernel<2, 16><<<b.grid, ColTile<2, 16>::THREADS, ColTile<2, 16>::SMEM_BYTES, st>>>(
+        *b.map_p, *b.map_uvw, g, kd);
+    return cudaGetLastError();
+  }
   if (a.dtype == FSLBM_F32) return launch_step2_t<float>(b, g, k, st);
   if (a.dtype == FSLBM_F16) return launch_step2_t<__half>(b, g, k, st);
   return cudaErrorInvalidValue;
