@@ -32,6 +32,11 @@ W = dict(lx=128, ly=128, lz=512, R=63.0, cx=63.5, cy=63.5, nu=0.0111, tblend=0.0
 PUBLISHED_MLUPS = 3790.0          # the reference's published FP32 D3Q27 FSLBM throughput
 E2E_INNER = 200                   # time steps per end-to-end solve request
 METRIC = "MLUPS (plain FSLBM step, all box cells)"
+# plain workload's storage types (--dtype): library type, bytes per value, step kernel, the
+# line's dtype (the arithmetic type; FP16 storage computes in FP32)
+STORAGE = {"f32": ("F32", 4, "fslbm_step2_kernel<2,32,packed>", "f32"),
+           "f64": ("F64", 8, "fslbm_col_kernel<2,16>", "f64"),
+           "f16": ("F16", 2, "fslbm_step2_kernel<2,32,packed,__half>", "f16 storage, f32 arithmetic")}
 
 
 def physics():
@@ -167,9 +172,10 @@ def seeded_start(O, planes, seed_offset=0):
                              seed=W["seed"] + seed_offset)
 
 
-def cpu_port_sample(seconds=10.0, planes=64, nthreads=0):
-    """The oracle's FP32 restatement of the reference step on the host cores, on a bounded
-    streamwise slice of the workload (same cross-section and parameters)."""
+def cpu_port_sample(seconds=10.0, planes=64, nthreads=0, dtype=np.float32):
+    """The oracle's restatement of the reference step (FP32, or FP64 for an FP64 line) on the
+    host cores, on a bounded streamwise slice of the workload (same cross-section and
+    parameters)."""
     O = _oracle()
     ub, umax, g = physics()
     f = seeded_start(O, planes)
@@ -178,20 +184,21 @@ def cpu_port_sample(seconds=10.0, planes=64, nthreads=0):
     prm = dict(tblend=W["tblend"], pin=0.0, nu=W["nu"], d1=W["d1"], blend=W["blend"],
                force=(0.0, 0.0, -g))
     threads = nthreads or O.threads()
-    f = f.astype(np.float32)
-    f, _ = O.run_core(m2, planes, f, prm, 1, monitor_every=50, radius=W["R"], dtype=np.float32,
+    f = f.astype(dtype)
+    f, _ = O.run_core(m2, planes, f, prm, 1, monitor_every=50, radius=W["R"], dtype=dtype,
                       nthreads=threads)                      # warm-up
     steps, t0 = 0, time.perf_counter()
     while True:
         f, _ = O.run_core(m2, planes, f, prm, 1, monitor_every=50, radius=W["R"],
-                          dtype=np.float32, nthreads=threads)
+                          dtype=dtype, nthreads=threads)
         steps += 1
         el = time.perf_counter() - t0
         if el >= seconds and steps >= 3:
             break
     cells = W["lx"] * W["ly"] * planes
     return {"value": cells * steps / el / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
-            "sample": f"{steps} FP32 steps of a {planes}-plane slice (128x128 cross-section) of "
+            "sample": f"{steps} {'FP64' if dtype == np.float64 else 'FP32'} steps of a {planes}-plane "
+                      f"slice (128x128 cross-section) of "
                       f"the workload, oracle restatement of FSLBM.cu with OpenMP"}, el / steps
 
 
@@ -255,11 +262,11 @@ def run_reference_arm(args, rank, world, local):
                force=(0.0, 0.0, -g))
     for _ in range(args.warmup):
         f, _ = O.run_core(m2, planes, f, prm, 1, monitor_every=50, radius=W["R"],
-                          dtype=np.float32, nthreads=threads)
+                          dtype=dtype, nthreads=threads)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         f, _ = O.run_core(m2, planes, f, prm, 1, monitor_every=50, radius=W["R"],
-                          dtype=np.float32, nthreads=threads)
+                          dtype=dtype, nthreads=threads)
     el = time.perf_counter() - t0
     cells = W["lx"] * W["ly"] * planes
     mlups = cells * args.steps / el / 1e6
@@ -291,7 +298,8 @@ def run_ours(args, rank, world, local):
                          buffer_depth=10)
     prm = fb.Params.make(tblend=W["tblend"], pin=0.0, nu=W["nu"], d1=W["d1"], delta=1,
                          blend=W["blend"], monitor_every=50, force=(0.0, 0.0, -g))
-    s = fb.Solve(ctx, dom, prm, fb.F32)
+    st_name, es, kernel_name, dtype_name = STORAGE[args.dtype]
+    s = fb.Solve(ctx, dom, prm, getattr(fb, st_name))
     f0 = fb.init_poiseuille(dom, umax, noise=1e-3, modes=4, mode_amp=0.1 * ub / umax,
                             seed=W["seed"] + rank)
     s.set_fields(f0)
@@ -359,24 +367,32 @@ def run_ours(args, rank, world, local):
     if rank == 0:
         peak, peak_kind = hbm_peak()
         kern_avg_ms = kern_ms / max(kern_n, 1)
-        alg_bytes = 32.0 * cells                  # read p,u,v,w + write p,u,v,w, FP32
+        alg_bytes = 8.0 * es * cells              # read p,u,v,w + write p,u,v,w
         achieved = alg_bytes / (kern_avg_ms * 1e-3) / 1e9
-        cpu, _ = cpu_port_sample(seconds=args.cpu_seconds) if args.cpu_seconds > 0 else (None, 0)
+        cpu, _ = (cpu_port_sample(seconds=args.cpu_seconds,
+                                  dtype=np.float64 if args.dtype == "f64" else np.float32)
+                  if args.cpu_seconds > 0 else (None, 0))
         value = world * cells * args.steps / (ms * 1e-3) / 1e6
         line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world,
                 "fluid_mlups": value * fluid_fraction(),
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": value / PUBLISHED_MLUPS, "dtype": "f32",
+                "vs_baseline": value / PUBLISHED_MLUPS if args.dtype == "f32" else None,
+                "dtype": dtype_name,
                 "data": "synthetic (seeded Poiseuille + random-phase modes)",
-                "config": workload_config(),
+                "config": workload_config() if args.dtype == "f32" else workload_config({
+                    "workload": f"plain FSLBM, {args.dtype.upper()} storage, periodic pipe 512 (z, "
+                                "streamwise) x 128 x 128, R=63, bulk Re 5300 body force, order-4 "
+                                "corrector, tblend 0.02",
+                    "l2": f"inputs larger than L2: 2 x {8 * es * cells / 2 / 1e6:.0f} MB state "
+                          "ping-pong vs 126 MB L2"}),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": None,
                              "traffic_note": "DRAM counters need a profiler, so the run does not "
                                              "measure them; per-launch DRAM bytes of ncu captures "
                                              "are in profiles/",
                              "peak_source": f"{peak_kind} hbm_gbs",
-                             "kernel": "fslbm_step2_kernel<2,32,packed>",
+                             "kernel": kernel_name,
                              "kernel_ms_avg": kern_avg_ms, "algorithmic_bytes": alg_bytes},
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "max_abs_u": umax_now}
@@ -742,6 +758,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--workload", default="plain", choices=["plain", "ensemble", "served", "mixed"])
+    ap.add_argument("--dtype", default="f32", choices=["f32", "f64", "f16"],
+                    help="plain workload: storage type of the solve (the default line is FP32)")
     ap.add_argument("--requests", type=int, default=1000, help="served workload: request count")
     ap.add_argument("--ensemble-dtype", default="f32", choices=["f32", "f16"],
                     help="ensemble workload: storage type of the batched members")
