@@ -587,14 +587,14 @@ def serve_stream(fb, wl, reqs, policy, round_cells=0):
 
 
 def run_served(args):
-    """Served solves: a seeded Poisson stream (200 req/s) of pipe solves (32^3 .. 256x96x96
-    cells, 200..5000 steps, Re 50..5000, FP32 or FP16 storage) submitted in real time to the
-    continuous-batching server under a 150 GB budget."""
+    """Served solves: a seeded Poisson stream (--rate, 200 requests/s by default) of pipe solves
+    (32^3 .. 256x96x96 cells, 200..5000 steps, Re 50..5000, FP32 or FP16 storage) submitted in
+    real time to the continuous-batching server under a 150 GB budget."""
     import flowcontrast_b200 as fb
     from flowcontrast_b200 import build, workloads as wl
     build.build()
     f32_only = args.served_dtype == "f32"
-    reqs = wl.request_stream(args.requests, rate=200.0, mixed_fraction=0.0 if f32_only else 0.5)
+    reqs = wl.request_stream(args.requests, rate=args.rate, mixed_fraction=0.0 if f32_only else 0.5)
     check = set(range(0, len(reqs), max(1, len(reqs) // 4)))     # requests checked afterwards
     srv = fb.Server(0, hbm_budget=int(150e9), quantum=50)
     # warm-up (kernel set-up and graph capture paths), not counted
@@ -671,7 +671,7 @@ def run_served(args):
             "unit": "MLUPS", "n_gpus": 1, "steps": len(reqs), "warmup": 4,
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if f32_only else "f32+f16", "data": "synthetic (seeded Poisson request stream)",
-            "config": {"workload": f"{len(reqs)} requests, Poisson 200/s, cells log-uniform "
+            "config": {"workload": f"{len(reqs)} requests, Poisson {args.rate:g}/s, cells log-uniform "
                                    "32^3..256x96x96, steps U[200,5000], Re log-uniform [50,5000], "
                                    + ("FP32 storage only" if f32_only else "FP32 or FP16 storage 50/50")
                                    + ", budget 150 GB, quantum 50",
@@ -761,6 +761,8 @@ def main():
     ap.add_argument("--dtype", default="f32", choices=["f32", "f64", "f16"],
                     help="plain workload: storage type of the solve (the default line is FP32)")
     ap.add_argument("--requests", type=int, default=1000, help="served workload: request count")
+    ap.add_argument("--rate", type=float, default=200.0,
+                    help="served workload: Poisson arrival rate (requests per second)")
     ap.add_argument("--ensemble-dtype", default="f32", choices=["f32", "f16"],
                     help="ensemble workload: storage type of the batched members")
     ap.add_argument("--served-dtype", default="mixed", choices=["mixed", "f32"],
