@@ -109,6 +109,31 @@ def test_batch_tile_heights_and_warp_shapes(built, ctx, monkeypatch, tile_y, sha
         s.close()
 
 
+def test_batch_fp64_members_step_alone(built, ctx):
+    """FP64 members do not enter the persistent launch (FP32 / FP16 storage only): the batch steps
+    them one after another through the FP64 column kernel, with each member's own result."""
+    fb = built
+    specs = member_specs(n=3, seed=11)
+    steps = 20
+    alone = []
+    for sp in specs:
+        s = make_member(fb, ctx, sp, dtype=fb.F64)
+        s.step(steps)
+        s.sync()
+        alone.append(s.get_fields(np.float64))
+        s.close()
+    members = [make_member(fb, ctx, sp, dtype=fb.F64) for sp in specs]
+    b = fb.Batch(ctx, members)
+    b.step(steps)
+    b.sync()
+    for s, want in zip(members, alone):
+        assert np.array_equal(s.get_fields(np.float64), want)
+        assert s.info()["steps"] == steps
+    b.close()
+    for s in members:
+        s.close()
+
+
 def test_batch_member_stops(built, ctx):
     """Members with different step budgets share launches; each stops at its own budget and
     equals the member stepped alone for that many steps."""
