@@ -227,3 +227,21 @@ def test_production_cross_section_slab_fp32(built, ctx):
     ep, eu, eps = errors(got, ref, m2)
     assert len(log) == 2
     assert eu <= 1e-5 and eps <= 1e-5, (ep, eu, eps)
+
+
+def test_production_cross_section_slab_fp64(built, ctx):
+    """The same slab in FP64 through the FP64 column kernel (32 x 16 tiles, 32 of them, several
+    streamwise chunks per tile in both march directions) against the FP64 oracle within 1e-12."""
+    lx = ly = 128
+    L, R = 64, 63.0
+    m2 = circle_mask(lx, ly, R, 63.5, 63.5)
+    dom = built.make_domain(lx, ly, L, radius=R, cx=63.5, cy=63.5, buffer_depth=10)
+    ub = 5300.0 * 0.0111 / (2 * R)
+    g = 2 * (180.0 * 0.0111 / R) ** 2 / R
+    f = built.init_poiseuille(dom, 2 * ub, noise=1e-3, modes=4, mode_amp=0.05, seed=78)
+    prm = dict(tblend=0.02, pin=0.0, nu=0.0111, d1=2, blend=1.0, force=(0.0, 0.0, -g))
+    ref, mon = O.run_core(m2, L, f, prm, 40, monitor_every=20, radius=R)
+    got, log = run_gpu(built, ctx, dom, prm, built.F64, f, 40, monitor_every=20)
+    ep, eu, eps = errors(got, ref, m2)
+    assert len(log) == 2
+    assert eu <= 1e-12 and eps <= 1e-12, (ep, eu, eps)
