@@ -10,11 +10,13 @@
 //    halo, u,v,w with the corrector's 2*d1 halo, as two TMA boxes per plane into a window of 8
 //    planes for TY = 32 (output plane .. 3 planes ahead for d1 = 2), 7 for TY = 16;
 //  - no block-wide barrier in the march and no producer thread: per-slot "full" mbarriers count
-//    TMA completion, each warp releases a slot after its last read of the plane in it, and the
-//    last warp to release a slot refills it, so warps drift within the window and none waits
-//    for a free slot;
+//    TMA completion, each warp releases the slots of a pair of planes after its last read of
+//    them, and the last warp to release a pair refills both slots, so warps drift within the
+//    window and none waits for a free slot;
 //  - the streamwise corrector taps behind the output plane come from a 2*d1 register history
-//    of the thread's own columns, the taps ahead from the window;
+//    of the thread's own columns, the taps ahead from the window; in the FP32 single-pipe
+//    kernel the output plane's own centre pairs come from the predictor's centre row of the
+//    same plane, read one iteration earlier;
 //  - grid = tiles x streamwise chunks in chunk-major order, so concurrent CTAs work at nearby
 //    planes and halos hit L2; odd chunks march downwards, so the planes two neighbouring
 //    chunks share are read by both at the same time;
