@@ -262,11 +262,11 @@ def run_reference_arm(args, rank, world, local):
                force=(0.0, 0.0, -g))
     for _ in range(args.warmup):
         f, _ = O.run_core(m2, planes, f, prm, 1, monitor_every=50, radius=W["R"],
-                          dtype=dtype, nthreads=threads)
+                          dtype=np.float32, nthreads=threads)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         f, _ = O.run_core(m2, planes, f, prm, 1, monitor_every=50, radius=W["R"],
-                          dtype=dtype, nthreads=threads)
+                          dtype=np.float32, nthreads=threads)
     el = time.perf_counter() - t0
     cells = W["lx"] * W["ly"] * planes
     mlups = cells * args.steps / el / 1e6

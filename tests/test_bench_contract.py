@@ -6,6 +6,7 @@ the oracle's, which must equal the library's fslbm_init_poiseuille bit for bit. 
 subprocess of the reference arm's set-up must not map libfslbm.so.
 """
 import os
+import json
 import subprocess
 import sys
 
@@ -47,6 +48,20 @@ def test_reference_arm_inputs_do_not_load_the_library():
     assert r.returncode == 0, r.stderr[-2000:]
     assert "liboracle.so" in r.stdout
     assert "libfslbm.so" not in r.stdout
+
+
+def test_reference_arm_runs_and_prints_its_line():
+    """`bench.py --impl reference` end to end on the host cores (no GPU needed for its timed
+    part): one JSON line with the reference arm's keys, and the solver library never loaded."""
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--steps", "1", "--warmup", "3"], capture_output=True, text=True, timeout=600,
+                       cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] in ("port", "reference")
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert line["config"] == bench.workload_config()
 
 
 def test_fluid_fraction_of_the_bench_pipe():
