@@ -100,7 +100,7 @@ extern "C" int fslbm_ctx_create(int device, fslbm_ctx** out) {
   cudaDeviceProp prop;
   CUDA_TRY(cudaGetDeviceProperties(&prop, device));
   if (prop.major != 10)
-    return fslbm_set_error(FSLBM_ERR_ARG, "ctx_create: device %d is sm_%d%d; this build targets sm_100a",
+    return fslbm_set_error(FSLBM_ERR_ARG, "ctx_create: device %d is sm_%d%d; the library is compiled for sm_100a",
                            device, prop.major, prop.minor);
   auto* c = new fslbm_ctx;
   c->device = device;
