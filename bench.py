@@ -396,10 +396,34 @@ def run_ours(args, rank, world, local):
                              "kernel_ms_avg": kern_avg_ms, "algorithmic_bytes": alg_bytes},
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "max_abs_u": umax_now}
+        if world == 1 and args.dtype == "f32" and not args.no_extras:
+            line.update(extra_measurements(args))
         print(json.dumps(line), flush=True)
     s.close()
     ctx.close()
     return 0
+
+
+def extra_measurements(args):
+    """Measured after the timed region of the single-GPU default line, on the same GPU: the
+    batched ensemble against the same pipes one at a time (500 steps each way), and the error of
+    each storage form against FP64 after 200 steps on the production pipe."""
+    import copy
+    a = copy.copy(args)
+    a.steps, a.warmup, a.ensemble_dtype, a.tuning_out = 500, 20, "f32", None
+    ens = ensemble_line(a)
+    mix = mixed_line(a)
+    return {
+        "ensemble": {"workload": ens["config"]["workload"], "members": ens["config"]["members"],
+                     "cells": ens["config"]["cells"], "steps": ens["steps"],
+                     "value": ens["value"], "unit": "MLUPS",
+                     "plain_one_at_a_time_mlups": ens["plain_one_at_a_time_mlups"],
+                     "speedup_vs_plain": ens["speedup_vs_plain"],
+                     "batch_equals_plain_bitwise": ens["batch_equals_plain_bitwise"],
+                     "kernel": ens["roofline"]["kernel"], "clocks": ens["clocks"]},
+        "precision": {"workload": mix["config"]["workload"],
+                      "errors_200_steps_vs_f64": mix["errors_200_steps"], "mlups": mix["mlups"]},
+    }
 
 
 # ------------------------------------------------------------------------------------------
@@ -419,10 +443,10 @@ def batch_kernel_name(storage):
     return f"fslbm_step2_batch_kernel<2,{ty},{form},{te}> (chained steps)"
 
 
-def run_ensemble(args):
+def ensemble_line(args):
     """Mixed-size ensemble (64 seeded pipes, L in [32,256], n in [24,96], Re in [50,3000]):
     the batched persistent launch (FP32 storage, or FP16 storage with --ensemble-dtype f16)
-    against the same pipes stepped one at a time by the plain FP32 method."""
+    against the same pipes stepped one at a time by the plain FP32 method. Returns its line."""
     import flowcontrast_b200 as fb
     from flowcontrast_b200 import build, workloads as wl
     build.build()
@@ -544,11 +568,15 @@ def run_ensemble(args):
                     "h2d_bytes_per_step": 16.0 * cells / args.steps,
                     "d2h_bytes_per_step": 16.0 * cells / args.steps},
             "gpu_launches": launches, "clocks": clocks}
-    print(json.dumps(line), flush=True)
     b.close()
     for s in solves:
         s.close()
     ctx.close()
+    return line
+
+
+def run_ensemble(args):
+    print(json.dumps(ensemble_line(args)), flush=True)
     return 0
 
 
@@ -693,9 +721,10 @@ def run_served(args):
     return 0
 
 
-def run_mixed(args):
+def mixed_line(args):
     """Storage precision on the production pipe (512x128x128, Re 500/2000/5300): error of the
-    FP32 and FP16-storage forms against the FP64 solve after 200 steps, and their step rates."""
+    FP32 and FP16-storage forms against the FP64 solve after 200 steps, and their step rates.
+    Returns its line."""
     import flowcontrast_b200 as fb
     from flowcontrast_b200 import build
     build.build()
@@ -745,7 +774,11 @@ def run_mixed(args):
             "vs_baseline": None, "dtype": "f16 storage, f32 arithmetic", "data": "synthetic",
             "config": {"workload": "512x128x128 pipe, R=63, tblend 0.02, d1 2, order 4, Re 500/2000/5300"},
             "errors_200_steps": out, "mlups": rates, "f16_gain_vs_f32": rates["f16"] / rates["f32"]}
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_mixed(args):
+    print(json.dumps(mixed_line(args)), flush=True)
     return 0
 
 
@@ -758,6 +791,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--workload", default="plain", choices=["plain", "ensemble", "served", "mixed"])
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default line: skip the ensemble and precision measurements after it")
     ap.add_argument("--dtype", default="f32", choices=["f32", "f64", "f16"],
                     help="plain workload: storage type of the solve (the default line is FP32)")
     ap.add_argument("--requests", type=int, default=1000, help="served workload: request count")
