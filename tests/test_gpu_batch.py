@@ -200,7 +200,21 @@ def test_autotune_restores_state_and_keeps_results(built, ctx, tmp_path):
     for s, (want, _) in zip(again, alone):
         assert np.array_equal(s.get_fields(np.float32), want)
     b2.close()
-    for s in members + again:
+    # a table in the earlier form ("warp16x4": 0 or 1, the same meaning as warp_shape 0 or 1) loads
+    old_form = str(tmp_path / "tiling_old.json")
+    with open(old_form, "w") as f:
+        f.write('{"format": "fslbm batch tiling 1", "classes": {' + ", ".join(
+            f'"{k}": {{"chunk": {v["chunk"]}, "warp16x4": {min(v["warp_shape"], 1)}, "trial_ms": 1.0}}'
+            for k, v in table.items()) + "}}")
+    third = [make_member(fb, ctx, sp) for sp in specs]
+    b3 = fb.Batch(ctx, third)
+    b3.load_tiling(old_form)
+    b3.step(steps)
+    b3.sync()
+    for s, (want, _) in zip(third, alone):
+        assert np.array_equal(s.get_fields(np.float32), want)
+    b3.close()
+    for s in members + again + third:
         s.close()
 
 
